@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""CW-FDTD benchmark: Gcell-updates/s of the B200 solver against its HBM roofline.
+
+Workload (default): the 2x2 MMI-like block, 321 x 161 x 101 cells (5.22 M) at
+0.025 um, 20-cell CPML, seeded projected design density, run to steady state at
+rtol = 1e-6 in the fp32 storage form.  One bench "step" is one complete CW solve
+(ramp, convergence probes every Tn steps, t0/t1 captures, 3-sample extraction).
+
+Reported in one JSON line (rank 0):
+  value       cell-updates / device time of the time-stepping (CUDA events on the
+              library's stream; materials already resident), summed over ranks
+              (each rank solves its own seeded replica: weak scaling)
+  e2e         the same metric through the public API ``FDTD.solve_forward`` with
+              host buffers: material upload, solve, complex-field download and
+              the source-power post-processing, wall clock
+  roofline    algorithmic bytes per time step (60 B per cell fp32 / 120 B fp64,
+              plus 32 / 64 B per cell and CPML slab) / average step time, against
+              the measured HBM copy bandwidth
+  fp64        the plain fp64 solve of the same problem and the fp32 error vs it
+  cpu_baseline  the reference C++ core (oracle/_ref/FDTD.so, compiled from the
+              reference sources) on the host cores, z-slab threads, bounded sample
+
+``--impl reference`` times that reference core alone (rank 0) on the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-updates/s (CW-FDTD, fp32 storage, MMI block 321x161x101, rtol=1e-6)"
+UNIT = "Gcell-updates/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--kernel", default="fused", choices=["fused", "unfused"])
+    ap.add_argument("--workload", default="mmi", choices=["mmi", "waveguide"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the fp64 comparison solve")
+    return ap.parse_args()
+
+
+def make_problem(workload: str, seed: int):
+    from emopt_b200 import problems as P
+    if workload == "mmi":
+        return P.mmi_block(seed=seed)
+    return P.waveguide(fixed_steps=None)
+
+
+def algorithmic_bytes_per_step(shape, w, word: int) -> int:
+    """Bulk: read E, H (6 words) and the 3 E-update coefficients, write E, H (6)
+    = 15 words per cell; each CPML slab a cell lies in adds 4 psi reads and 4
+    psi writes.  The z-max slab has w-1 active planes (strict comparison)."""
+    Nz, Ny, Nx = shape
+    n = Nz * Ny * Nx
+    slab = (Nz * Ny * (min(w[0], Nx) + min(w[1], Nx)) + Nz * Nx * (min(w[2], Ny) + min(w[3], Ny))
+            + Ny * Nx * (min(w[4], Nz) + max(min(w[5], Nz) - 1, 0)))
+    return word * (15 * n + 8 * slab)
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+            os.unlink(self.path)
+        except Exception:
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if sm:
+            out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(mx), samples=len(sm),
+                       reasons=sorted(reasons))
+        return out
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier_max(values: list[float], world: int):
+    """Max over ranks of each value (device-timed seconds)."""
+    if world == 1:
+        return values
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def barrier_sum(values: list[float], world: int):
+    if world == 1:
+        return values
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.tolist()
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(p, budget_s: float = 12.0):
+    """Reference core on the host cores (z-slab threads), bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import oracle_for
+    from oracle import driver
+    kind = "reference" if driver.available("ref") else "port"
+    lib = "ref" if kind == "reference" else "oracle"
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except Exception:
+        cores = os.cpu_count() or 1
+    o = oracle_for(p, lib)
+    t_cal = o.run_fixed_slabs(0, cores, time_only_steps=2)
+    steps = max(2, int(budget_s / max(t_cal / 2, 1e-6)))
+    steps = min(steps, 400)
+    o = oracle_for(p, lib)
+    t = o.run_fixed_slabs(0, cores, time_only_steps=steps)
+    gcells = p.ncells * steps / t / 1e9
+    return {"value": gcells, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{steps} time steps of {p.name} (fp64, reference arithmetic), "
+                      f"{cores} z-slab threads, {t:.1f} s"}
+
+
+def run_reference(args):
+    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    p = make_problem(args.workload, 0)
+    for _ in range(args.warmup):
+        cpu_baseline(p, budget_s=2.0)
+    vals = [cpu_baseline(p, budget_s=12.0) for _ in range(args.steps)]
+    v = statistics.median([x["value"] for x in vals])
+    base = dict(vals[0])
+    base["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": p.name, "cells": p.ncells, "precision": "fp64 (reference)",
+                       "sample": base["sample"]},
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    world, rank, local = dist_setup(args.gpus)
+    from emopt_b200 import problems as P
+    p = make_problem(args.workload, seed=rank)
+    sim = P.make_solver(p, precision=args.precision, kernel=args.kernel, device=local)
+    t0 = [sim._Ex_fwd_t0, sim._Ey_fwd_t0, sim._Ez_fwd_t0, sim._Hx_fwd_t0, sim._Hy_fwd_t0,
+          sim._Hz_fwd_t0]
+    t1 = [sim._Ex_fwd_t1, sim._Ey_fwd_t1, sim._Ez_fwd_t1, sim._Hx_fwd_t1, sim._Hy_fwd_t1,
+          sim._Hz_fwd_t1]
+    for _ in range(max(args.warmup, 1)):
+        sim._solve(t0, t1, sim._sources)
+    barrier(world)
+    # ---- device-timed region: K complete solves, inputs resident
+    infos = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            infos.append(sim._solve(t0, t1, sim._sources))
+    barrier(world)
+    dev_s = sum(i["device_ms"] for i in infos) / 1e3
+    steps_total = sum(i["steps"] for i in infos)
+    launches = sum(i.get("launches", 0) for i in infos)
+    cell_updates = float(p.ncells) * steps_total
+    (dev_s_max,) = barrier_max([dev_s], world)
+    (cell_updates_all,) = barrier_sum([cell_updates], world)
+    value = cell_updates_all / dev_s_max / 1e9
+    fields32 = np.stack([sim._raw(c, False).copy() for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")])
+
+    # ---- e2e: public API with host buffers (materials re-uploaded each call)
+    barrier(world)
+    wall = []
+    for _ in range(args.steps):
+        sim._materials_dirty = True
+        t_a = time.perf_counter()
+        sim.solve_forward()
+        wall.append(time.perf_counter() - t_a)
+    (wall_max,) = barrier_max([sum(wall)], world)
+    e2e_steps = sim.last_solve["steps"] * args.steps
+    (e2e_updates,) = barrier_sum([float(p.ncells) * e2e_steps], world)
+    src_bytes = sum(6 * a[0].size * 16 for a, *_ in p.sources)
+    h2d = 6 * p.ncells * 16 + src_bytes
+    d2h = 6 * p.ncells * 16
+
+    # ---- roofline of the step kernel
+    word = 4 if args.precision == "fp32" else 8
+    alg = algorithmic_bytes_per_step(p.shape, p.w_pml, word)
+    step_s = dev_s / steps_total
+    peak, peak_kind = measured_peak()
+    achieved = alg / step_s / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"traffic_{args.kernel}_{args.precision}_{p.name}.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    result = None
+    if rank == 0:
+        line = {
+            "metric": METRIC if (args.workload == "mmi" and args.precision == "fp32") else
+            f"Gcell-updates/s ({args.workload}, {args.precision})",
+            "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * dev_s_max / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+            "config": {"workload": p.name, "cells": p.ncells, "time_steps_per_solve":
+                       infos[-1]["steps"], "rtol": p.rtol, "kernel": args.kernel,
+                       "precision": args.precision, "parallelism": f"replicas{world}",
+                       "l2": "working set %.0f MB > 126 MB L2; no flush needed" %
+                             ((2 * 6 + 3) * word * p.ncells / 1e6)},
+            "e2e": {"value": round(e2e_updates / wall_max / 1e9, 3), "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "alg_bytes_per_step": alg, "step_us": round(step_s * 1e6, 2)},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        result = line
+    # ---- fp64 comparison solve (not in the timed region)
+    if rank == 0 and not args.no_fp64 and args.precision == "fp32":
+        sim64 = P.make_solver(p, precision="fp64", kernel=args.kernel, device=local)
+        info64 = sim64._solve([sim64._Ex_fwd_t0, sim64._Ey_fwd_t0, sim64._Ez_fwd_t0,
+                               sim64._Hx_fwd_t0, sim64._Hy_fwd_t0, sim64._Hz_fwd_t0],
+                              [sim64._Ex_fwd_t1, sim64._Ey_fwd_t1, sim64._Ez_fwd_t1,
+                               sim64._Hx_fwd_t1, sim64._Hy_fwd_t1, sim64._Hz_fwd_t1],
+                              sim64._sources)
+        f64 = np.stack([sim64._raw(c, False) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")])
+        err = float(np.linalg.norm(fields32 - f64) / np.linalg.norm(f64))
+        alg64 = algorithmic_bytes_per_step(p.shape, p.w_pml, 8)
+        step64 = info64["device_ms"] / 1e3 / info64["steps"]
+        result["fp64"] = {"value": round(p.ncells * info64["steps"] / (info64["device_ms"] / 1e3) / 1e9, 3),
+                          "steps": info64["steps"], "fp32_steps": infos[-1]["steps"],
+                          "fp32_rel_l2_vs_fp64": err,
+                          "roofline_frac": round(alg64 / step64 / 1e9 / peak, 4),
+                          "speedup_fp32_over_fp64": round(value / (p.ncells * info64["steps"] /
+                                                                   (info64["device_ms"] / 1e3) / 1e9), 3)}
+        del sim64
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            result["cpu_baseline"] = cpu_baseline(p)
+        except Exception as e:  # the baseline is reported, never required
+            result["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",
+                                      "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

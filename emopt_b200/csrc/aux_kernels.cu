@@ -1,0 +1,237 @@
+// aux_kernels.cu -- set-up, extraction and convergence kernels of the
+// device-resident CW solve.
+#include "kernels.h"
+
+namespace fdtdb {
+
+namespace {
+
+unsigned blocks_for(long long n, int tpb) { return (unsigned)((n + tpb - 1) / tpb); }
+
+// E-update coefficients of one cell (src/fdtd.cpp:513-552) in fp64.
+__device__ __forceinline__ void eps_ab(c128 e, double dt, bool lossy, double& a, double& b) {
+    if (!lossy) {
+        a = 1.0;
+        b = dt / e.real;
+    } else {
+        double rdt = e.real * (1.0 / dt), ih = e.imag * 0.5;
+        a = (rdt - ih) / (rdt + ih);
+        b = 1.0 / (rdt + ih);
+    }
+}
+
+template <typename T>
+__global__ void k_material_coeffs(const c128* eps, const c128* mu, int Nx, int Ny, int Nz, int px,
+                                  double dt, bool lossy, T* b_out, T* a_out, T* bH_out) {
+    long long n = (long long)Nx * Ny * Nz;
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    int k = (int)(g % Nx);
+    long long row = g / Nx;  // i*Ny + j
+    long long p = row * px + k;
+    if (eps) {
+        double a, b;
+        eps_ab(eps[g], dt, lossy, a, b);
+        b_out[p] = T(b);
+        if (a_out) a_out[p] = T(a);
+    }
+    if (mu) bH_out[p] = T(dt / mu[g].real);
+}
+
+__global__ void k_uniform_check(const c128* mu, long long n, int* flag) {
+    double ref = mu[0].real;
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n;
+         g += (long long)gridDim.x * blockDim.x)
+        if (mu[g].real != ref) { *flag = 0; return; }
+}
+
+template <typename T>
+__global__ void k_source_coeffs(const c128* ap, int i0, int j0, int k0, int I, int J, int K,
+                                const T* coef_arr, double coef_scalar, int Ny, int px, T* out) {
+    long long n = (long long)I * J * K;
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    int lk = (int)(q % K), lj = (int)((q / K) % J), li = (int)(q / ((long long)K * J));
+    long long p = ((long long)(li + i0) * Ny + (lj + j0)) * px + (lk + k0);
+    double coef = coef_arr ? (double)coef_arr[p] : coef_scalar;
+    c128 v = ap[q];
+    // sin(t + phase) = sin t cos(phase) + cos t sin(phase)
+    out[2 * q] = T(v.real * coef * cos(v.imag));
+    out[2 * q + 1] = T(v.real * coef * sin(v.imag));
+}
+
+template <typename T>
+__global__ void k_extract_3t(const T* t0, const T* t1, const T* cur, int Nx, long long n, int px,
+                             Fit3 fit, c128* out) {
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    long long p = (g / Nx) * px + (g % Nx);
+    out[g] = phasor_3t(fit, (double)t0[p], (double)t1[p], (double)cur[p]);
+}
+
+// Dense copy of one pitched snapshot into .real of complex128 values.
+template <typename T>
+__global__ void k_snapshot_real(const T* snap, int Nx, long long n, int px, c128* out) {
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    out[g].real = (double)snap[(g / Nx) * px + (g % Nx)];
+}
+
+// (re, im) -> (|z|, -atan2(im, re)), zero kept as (0, 0) (src/fdtd.cpp:1517-1576).
+__global__ void k_amp_phase(c128* a, long long n) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    double re = a[q].real, im = a[q].imag;
+    a[q].real = sqrt(re * re + im * im);
+    a[q].imag = (im == 0 && re == 0) ? 0.0 : -1 * atan2(im, re);
+}
+
+// Per-step source constants: (S, C) = env(t)(sin t, cos t) at t = n dt for the
+// H half-step and t = (n + 1/2) dt for the E half-step.
+__global__ void k_step_table(double4* tab, long long nsteps, double dt, double T, double m,
+                             double kk) {
+    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nsteps) return;
+    double tH = (double)n * dt, tE = ((double)n + 0.5) * dt;
+    double eH = src_envelope(tH, T, m, kk), eE = src_envelope(tE, T, m, kk);
+    double sH, cH, sE, cE;
+    sincos(tH, &sH, &cH);
+    sincos(tE, &sE, &cE);
+    tab[n] = make_double4(eH * sH, eH * cH, eE * sE, eE * cE);
+}
+
+__global__ void k_set_ll(long long* p, long long v) { *p = v; }
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One CTA.  Window shift and per-point refit follow emopt/fdtd.py:1072-1121;
+// the change norms ||A1-A0||/||A0|| and ||phi1-phi0||/||phi0|| follow
+// :1137-1138 and are reduced with warp shuffles, then across warps in smem.
+template <typename T>
+__global__ void __launch_bounds__(256) k_probe(const T* Ex, const T* Ey, const T* Ez, ProbeDev pd,
+                                               long long* step_base, int last_off,
+                                               long long advance, double dt) {
+    __shared__ double red[4][8];
+    __shared__ double tt[3];
+    long long nprobe = *step_base + last_off;
+    if (threadIdx.x == 0) {
+        pd.times[0] = pd.times[1];
+        pd.times[1] = pd.times[2];
+        pd.times[2] = (double)nprobe * dt;
+        tt[0] = pd.times[0]; tt[1] = pd.times[1]; tt[2] = pd.times[2];
+    }
+    __syncthreads();
+    double sdA = 0, sA0 = 0, sdP = 0, sP0 = 0;
+    const T* E[3] = {Ex, Ey, Ez};
+    for (int q = threadIdx.x; q < pd.nconv; q += blockDim.x) {
+        double phi0 = pd.phi[pd.nconv + q], A0 = pd.A[pd.nconv + q];
+        long long off = pd.map[q];
+        double phs = 0, amps = 0;
+        double ph[3], am[3];
+        for (int c = 0; c < 3; c++) {
+            double* w = pd.win + (long long)c * 3 * pd.nconv;
+            double w0 = w[pd.nconv + q], w1 = w[2 * pd.nconv + q];
+            double w2 = off >= 0 ? (double)E[c][off] : 0.0;
+            w[q] = w0; w[pd.nconv + q] = w1; w[2 * pd.nconv + q] = w2;
+            double f = phase_3t(tt[0], tt[1], tt[2], w0, w1, w2);
+            double a = amplitude_3t(tt[0], tt[1], tt[2], w0, w1, w2, f);
+            if (a < 0) { a *= -1; f += M_PI; }
+            ph[c] = f; am[c] = a;
+        }
+        phs = ph[0] + ph[1] + ph[2];
+        amps = am[0] + am[1] + am[2];
+        pd.phi[q] = phi0; pd.A[q] = A0;
+        pd.phi[pd.nconv + q] = phs; pd.A[pd.nconv + q] = amps;
+        double dA = amps - A0, dP = phs - phi0;
+        sdA += dA * dA; sA0 += A0 * A0; sdP += dP * dP; sP0 += phi0 * phi0;
+    }
+    sdA = warp_sum(sdA); sA0 = warp_sum(sA0); sdP = warp_sum(sdP); sP0 = warp_sum(sP0);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { red[0][wid] = sdA; red[1][wid] = sA0; red[2][wid] = sdP; red[3][wid] = sP0; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s[4] = {0, 0, 0, 0};
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+            for (int r = 0; r < 4; r++) s[r] += red[r][w];
+        pd.out[0] = sqrt(s[0]) / sqrt(s[1]);
+        pd.out[1] = sqrt(s[2]) / sqrt(s[3]);
+        pd.out[2] = pd.out[2] + 1.0;
+        *step_base = *step_base + advance;
+    }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_material_coeffs(const c128* eps, const c128* mu, int Nx, int Ny, int Nz, int px,
+                            double dt, bool lossy, T* b_out, T* a_out, T* bH_out,
+                            cudaStream_t st) {
+    long long n = (long long)Nx * Ny * Nz;
+    k_material_coeffs<T><<<blocks_for(n, 256), 256, 0, st>>>(eps, mu, Nx, Ny, Nz, px, dt, lossy,
+                                                             b_out, a_out, bH_out);
+}
+
+void launch_uniform_check(const c128* mu, long long n, int* flag, cudaStream_t st) {
+    k_uniform_check<<<296, 256, 0, st>>>(mu, n, flag);
+}
+
+template <typename T>
+void launch_source_coeffs(const c128* ap, int i0, int j0, int k0, int I, int J, int K,
+                          const T* coef_arr, double coef_scalar, int Ny, int px, T* out,
+                          cudaStream_t st) {
+    long long n = (long long)I * J * K;
+    if (n > 0)
+        k_source_coeffs<T><<<blocks_for(n, 256), 256, 0, st>>>(ap, i0, j0, k0, I, J, K, coef_arr,
+                                                               coef_scalar, Ny, px, out);
+}
+
+template <typename T>
+void launch_extract_3t(const T* t0, const T* t1, const T* cur, int Nx, int Ny, int Nz, int px,
+                       Fit3 fit, c128* out, cudaStream_t st) {
+    long long n = (long long)Nx * Ny * Nz;
+    k_extract_3t<T><<<blocks_for(n, 256), 256, 0, st>>>(t0, t1, cur, Nx, n, px, fit, out);
+}
+
+template <typename T>
+void launch_snapshot_real(const T* snap, int Nx, int Ny, int Nz, int px, c128* out,
+                          cudaStream_t st) {
+    long long n = (long long)Nx * Ny * Nz;
+    k_snapshot_real<T><<<blocks_for(n, 256), 256, 0, st>>>(snap, Nx, n, px, out);
+}
+
+void launch_amp_phase(c128* a, long long n, cudaStream_t st) {
+    if (n > 0) k_amp_phase<<<blocks_for(n, 256), 256, 0, st>>>(a, n);
+}
+
+void launch_step_table(double4* tab, long long nsteps, double dt, double T, double m, double kk,
+                       cudaStream_t st) {
+    if (nsteps > 0) k_step_table<<<blocks_for(nsteps, 256), 256, 0, st>>>(tab, nsteps, dt, T, m, kk);
+}
+
+void launch_set_ll(long long* p, long long v, cudaStream_t st) { k_set_ll<<<1, 1, 0, st>>>(p, v); }
+
+template <typename T>
+void launch_probe(const T* Ex, const T* Ey, const T* Ez, ProbeDev pd, long long* step_base,
+                  int last_off, long long advance, double dt, cudaStream_t st) {
+    k_probe<T><<<1, 256, 0, st>>>(Ex, Ey, Ez, pd, step_base, last_off, advance, dt);
+}
+
+#define INST(T)                                                                                 \
+    template void launch_material_coeffs<T>(const c128*, const c128*, int, int, int, int,       \
+                                            double, bool, T*, T*, T*, cudaStream_t);            \
+    template void launch_source_coeffs<T>(const c128*, int, int, int, int, int, int, const T*,   \
+                                          double, int, int, T*, cudaStream_t);                  \
+    template void launch_extract_3t<T>(const T*, const T*, const T*, int, int, int, int, Fit3,  \
+                                       c128*, cudaStream_t);                                    \
+    template void launch_snapshot_real<T>(const T*, int, int, int, int, c128*, cudaStream_t);   \
+    template void launch_probe<T>(const T*, const T*, const T*, ProbeDev, long long*, int,      \
+                                  long long, double, cudaStream_t);
+INST(float)
+INST(double)
+#undef INST
+
+}  // namespace fdtdb

@@ -1,0 +1,157 @@
+/*
+ * emopt_fdtd.h -- C ABI of the B200 CW-FDTD library (emopt_b200/FDTD.so).
+ *
+ * The first block is the reference library's ABI, symbol for symbol: the same
+ * names, argument order, argument meaning and (void) error behaviour as
+ * src/fdtd.hpp:571-643 (definitions src/fdtd.cpp:1618-1929), so that the
+ * reference binding emopt/fdtd_ctypes.py:26-149 loads this library unchanged.
+ * Caller arrays are retained by pointer exactly as in the reference; each
+ * per-call entry point reads them, computes on the GPU and writes the results
+ * back before returning.
+ *
+ * The second block adds what the reference does not have: an explicit
+ * destructor, error reporting, a precision switch and FDTD_solve_cw, which runs
+ * the whole time loop of emopt/fdtd.py:994-1194 on the device and only moves
+ * the materials in and the complex steady-state fields out.
+ *
+ * Layouts (reference conventions): padded local field arrays
+ * (I+2)(J+2)(K+2) doubles, x fastest; material, snapshot and source arrays
+ * unpadded I*J*K complex128 values {real, imag}.
+ */
+#ifndef EMOPT_FDTD_H
+#define EMOPT_FDTD_H
+
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct FDTDHandle FDTDHandle;
+typedef struct { double real, imag; } fdtd_complex128;   /* src/fdtd.hpp:22-80 */
+
+/* ----------------------------------------------- reference ABI (32 symbols) */
+FDTDHandle *FDTD_new(void);                                          /* src/fdtd.hpp:572, src/fdtd.cpp:1618 */
+void FDTD_set_wavelength(FDTDHandle *h, double wavelength);          /* src/fdtd.hpp:575, src/fdtd.cpp:1623 */
+void FDTD_set_physical_dims(FDTDHandle *h, double X, double Y, double Z,
+                            double dx, double dy, double dz);        /* src/fdtd.hpp:576, src/fdtd.cpp:1628 */
+void FDTD_set_grid_dims(FDTDHandle *h, int Nx, int Ny, int Nz);     /* src/fdtd.hpp:579, src/fdtd.cpp:1635 */
+void FDTD_set_local_grid(FDTDHandle *h, int k0, int j0, int i0,
+                         int K, int J, int I);                      /* src/fdtd.hpp:580, src/fdtd.cpp:1640 */
+void FDTD_set_dt(FDTDHandle *h, double dt);                         /* src/fdtd.hpp:583, src/fdtd.cpp:1648 */
+void FDTD_set_complex_eps(FDTDHandle *h, bool complex_eps);         /* src/fdtd.hpp:584, src/fdtd.cpp:1653 */
+void FDTD_set_field_arrays(FDTDHandle *h, double *Ex, double *Ey, double *Ez,
+                           double *Hx, double *Hy, double *Hz);     /* src/fdtd.hpp:585, src/fdtd.cpp:1658 */
+void FDTD_set_mat_arrays(FDTDHandle *h,
+                         fdtd_complex128 *eps_x, fdtd_complex128 *eps_y, fdtd_complex128 *eps_z,
+                         fdtd_complex128 *mu_x, fdtd_complex128 *mu_y, fdtd_complex128 *mu_z);
+                                                                     /* src/fdtd.hpp:589, src/fdtd.cpp:1665 */
+void FDTD_update_H(FDTDHandle *h, int n, double t);                 /* src/fdtd.hpp:593, src/fdtd.cpp:1672 */
+void FDTD_update_E(FDTDHandle *h, int n, double t);                 /* src/fdtd.hpp:594, src/fdtd.cpp:1677 */
+void FDTD_set_pml_widths(FDTDHandle *h, int xmin, int xmax, int ymin, int ymax,
+                         int zmin, int zmax);                        /* src/fdtd.hpp:597, src/fdtd.cpp:1682 */
+void FDTD_set_pml_properties(FDTDHandle *h, double sigma, double alpha,
+                             double kappa, double pow);              /* src/fdtd.hpp:600, src/fdtd.cpp:1689 */
+void FDTD_build_pml(FDTDHandle *h);                                  /* src/fdtd.hpp:602, src/fdtd.cpp:1695 */
+void FDTD_reset_pml(FDTDHandle *h);                                  /* src/fdtd.hpp:603, src/fdtd.cpp:1700 */
+void FDTD_set_t0_arrays(FDTDHandle *h,
+                        fdtd_complex128 *Ex_t0, fdtd_complex128 *Ey_t0, fdtd_complex128 *Ez_t0,
+                        fdtd_complex128 *Hx_t0, fdtd_complex128 *Hy_t0, fdtd_complex128 *Hz_t0);
+                                                                     /* src/fdtd.hpp:606, src/fdtd.cpp:1705 */
+void FDTD_set_t1_arrays(FDTDHandle *h,
+                        fdtd_complex128 *Ex_t1, fdtd_complex128 *Ey_t1, fdtd_complex128 *Ez_t1,
+                        fdtd_complex128 *Hx_t1, fdtd_complex128 *Hy_t1, fdtd_complex128 *Hz_t1);
+                                                                     /* src/fdtd.hpp:609, src/fdtd.cpp:1712 */
+double FDTD_calc_phase_2T(double t0, double t1, double f0, double f1);             /* src/fdtd.hpp:613, src/fdtd.cpp:1719 */
+double FDTD_calc_amplitude_2T(double t0, double t1, double f0, double f1,
+                              double phase);                                       /* src/fdtd.hpp:614, src/fdtd.cpp:1724 */
+double FDTD_calc_phase_3T(double t0, double t1, double t2, double f0, double f1,
+                          double f2);                                              /* src/fdtd.hpp:616, src/fdtd.cpp:1729 */
+double FDTD_calc_amplitude_3T(double t0, double t1, double t2, double f0, double f1,
+                              double f2, double phase);                            /* src/fdtd.hpp:617, src/fdtd.cpp:1734 */
+void FDTD_capture_t0_fields(FDTDHandle *h);                          /* src/fdtd.hpp:619, src/fdtd.cpp:1739 */
+void FDTD_capture_t1_fields(FDTDHandle *h);                          /* src/fdtd.hpp:620, src/fdtd.cpp:1744 */
+void FDTD_calc_complex_fields_2T(FDTDHandle *h, double t0, double t1);             /* src/fdtd.hpp:621, src/fdtd.cpp:1750 */
+void FDTD_calc_complex_fields_3T(FDTDHandle *h, double t0, double t1, double t2);  /* src/fdtd.hpp:622, src/fdtd.cpp:1755 */
+void FDTD_add_source(FDTDHandle *h,
+                     fdtd_complex128 *Jx, fdtd_complex128 *Jy, fdtd_complex128 *Jz,
+                     fdtd_complex128 *Mx, fdtd_complex128 *My, fdtd_complex128 *Mz,
+                     int i0, int j0, int k0, int I, int J, int K,
+                     bool calc_phase);                               /* src/fdtd.hpp:625, src/fdtd.cpp:1760 */
+void FDTD_clear_sources(FDTDHandle *h);                              /* src/fdtd.hpp:630, src/fdtd.cpp:1768 */
+void FDTD_set_source_properties(FDTDHandle *h, double src_T, double src_min);
+                                                                     /* src/fdtd.hpp:632, src/fdtd.cpp:1773 */
+double FDTD_src_func_t(FDTDHandle *h, int n, double t, double phase);/* src/fdtd.hpp:634, src/fdtd.cpp:1778 */
+void FDTD_set_bc(FDTDHandle *h, char *newbc);                        /* src/fdtd.hpp:637, src/fdtd.cpp:1783 */
+void FDTD_copy_to_ghost_comm(double *src, fdtd_complex128 *ghost, int I, int J, int K);
+                                                                     /* src/fdtd.hpp:640, src/fdtd.cpp:1789 */
+void FDTD_copy_from_ghost_comm(double *dest, fdtd_complex128 *ghost, int I, int J, int K);
+                                                                     /* src/fdtd.hpp:641, src/fdtd.cpp:1860 */
+
+/* ---------------------------------------------------------------- additions */
+
+/* Status codes returned by the additions and kept by FDTD_last_error. */
+enum {
+    FDTD_OK = 0,
+    FDTD_ERR_CUDA = 1,        /* a CUDA call failed (message in FDTD_last_error) */
+    FDTD_ERR_ARG = 2,         /* invalid argument or configuration */
+    FDTD_ERR_NODEVICE = 3,    /* no CUDA device visible */
+    FDTD_NMAX = 4,            /* FDTD_solve_cw: step budget Nmax exhausted before convergence */
+    FDTD_NONFINITE = 5        /* FDTD_solve_cw: the probe saw NaN/Inf when the budget ran out */
+};
+
+/* Releases the handle and its device memory.  The reference has no
+ * destructor (src/fdtd.cpp:1618-1621 allocates with no matching delete). */
+void FDTD_delete(FDTDHandle *h);
+
+/* Last status of the handle; copies its message into buf (NUL-terminated). */
+int FDTD_last_error(FDTDHandle *h, char *buf, int buflen);
+
+/* Selects the CUDA device of the handle (default: the calling thread's current
+ * device).  Must precede the first call that touches the device. */
+int FDTD_set_device(FDTDHandle *h, int device);
+
+/* Storage/arithmetic precision of FDTD_solve_cw: 64 (default, the reference's
+ * float64) or 32 (fields, coefficients and CPML state in float32; the
+ * steady-state fit, probes and outputs stay float64).  Returns a status. */
+int FDTD_set_precision(FDTDHandle *h, int bits);
+
+/* Time-stepping kernel of FDTD_solve_cw: 0 = fused one-launch-per-step kernel
+ * (default), 1 = separate H and E kernels. */
+int FDTD_set_kernel(FDTDHandle *h, int which);
+
+typedef struct {
+    long long Tn;              /* probe period and extraction spacing: int64(Ncycle*3/4) (emopt/fdtd.py:1021) */
+    double Nmax;               /* step budget: the loop stops once n > Nmax (emopt/fdtd.py:1054) */
+    double rtol;               /* amplitude tolerance; the phase tolerance is sqrt(rtol) (emopt/fdtd.py:1046-1047) */
+    const long long *conv_pts; /* probe indices into the padded local E arrays (emopt/fdtd.py:411-413) */
+    int nconv;
+    long long fixed_steps;     /* > 0: run exactly this many main steps without a convergence test */
+    int materials_unchanged;   /* 1: reuse the coefficients of the previous solve on this handle */
+    int copy_t1;               /* 1: also write the t1 snapshot into .real of the t1 arrays */
+} FDTDSolveOptions;
+
+typedef struct {
+    long long n_main;          /* steps of the main loop (index of the t0 capture) */
+    long long steps;           /* total time steps = n_main + 2*Tn */
+    double A_change;           /* last amplitude change norm */
+    double phi_change;         /* last phase change norm */
+    long long nprobes;         /* number of convergence probes */
+    double device_ms;          /* device time of all time steps (CUDA events) */
+    double total_ms;           /* device time of the whole call incl. transfers */
+    long long launches;        /* kernels this call launched */
+    int status;                /* FDTD_OK, FDTD_NMAX or FDTD_NONFINITE */
+} FDTDSolveResult;
+
+/* Device-resident CW solve: equivalent to FDTD_reset_pml, zeroing the fields
+ * and the loop of emopt/fdtd.py:1016-1194 (probe window, norm test, capture of
+ * t0 and t1 Tn steps apart, 3-sample extraction), run on the GPU.  Reads the
+ * material arrays and the sources registered with FDTD_add_source; writes the
+ * complex steady-state fields into the t0 arrays.  Returns a status. */
+int FDTD_solve_cw(FDTDHandle *h, const FDTDSolveOptions *opt, FDTDSolveResult *res);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EMOPT_FDTD_H */

@@ -1,0 +1,90 @@
+"""CPU tests of the C-ABI library: it loads without a GPU, exports every symbol
+declared in include/emopt_fdtd.h, keeps the reference's ctypes signatures, and
+its pure scalar entry points agree with the reference's known answers."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from helpers import ROOT, golden
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "emopt_fdtd.h")).read()
+    return sorted(set(re.findall(r"\b(FDTD_[A-Za-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_header_symbols():
+    from emopt_b200 import fdtd_ctypes as ct
+    lib = ctypes.CDLL(ct.so_path)
+    syms = header_symbols()
+    assert len(syms) == 38
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert set(ct.REFERENCE_SYMBOLS) | set(ct.ADDED_SYMBOLS) == set(syms)
+
+
+def test_reference_binding_loads_unchanged():
+    """The reference ctypes argtypes (emopt/fdtd_ctypes.py) bind to this library."""
+    from emopt_b200 import fdtd_ctypes as ct
+    assert len(ct.REFERENCE_SYMBOLS) == 32
+    for name in ct.REFERENCE_SYMBOLS:
+        fn = getattr(ct.libFDTD, name)
+        assert fn.argtypes is not None
+
+
+def test_struct_layouts():
+    from emopt_b200 import fdtd_ctypes as ct
+    assert ctypes.sizeof(ct.SolveOptions) == 56
+    assert ctypes.sizeof(ct.SolveResult) == 72
+
+
+def test_scalar_entry_points_match_reference_kat():
+    from emopt_b200 import fdtd_ctypes as ct
+    lib = ct.libFDTD
+    g = golden("kat_fit.npz")
+    t, f = g["t"], g["f"]
+    ph3 = np.array([lib.FDTD_calc_phase_3T(*t[q], *f[q]) for q in range(len(t))])
+    am3 = np.array([lib.FDTD_calc_amplitude_3T(*t[q], *f[q], g["phase3"][q]) for q in range(len(t))])
+    ph2 = np.array([lib.FDTD_calc_phase_2T(t[q, 0], t[q, 1], f[q, 0], f[q, 1]) for q in range(len(t))])
+    am2 = np.array([lib.FDTD_calc_amplitude_2T(t[q, 0], t[q, 1], f[q, 0], f[q, 1], g["phase2"][q])
+                    for q in range(len(t))])
+    # same formulas, same libm on the host: identical
+    np.testing.assert_array_equal(ph3, g["phase3"])
+    np.testing.assert_array_equal(am3, g["amp3"])
+    np.testing.assert_array_equal(ph2, g["phase2"])
+    np.testing.assert_array_equal(am2, g["amp2"])
+    h = lib.FDTD_new()
+    lib.FDTD_set_source_properties(h, float(g["src_T"]), float(g["src_min"]))
+    vals = [lib.FDTD_src_func_t(h, q, g["src_t"][q], g["src_phase"][q]) for q in range(len(g["src_t"]))]
+    np.testing.assert_array_equal(vals, g["src_value"])
+    lib.FDTD_delete(h)
+
+
+def test_no_device_fails_loudly():
+    """Without a GPU the handle reports FDTD_ERR_NODEVICE and the Python class raises."""
+    from conftest import has_cuda
+    if has_cuda():
+        pytest.skip("a CUDA device is present")
+    from emopt_b200 import fdtd_ctypes as ct
+    from emopt_b200 import problems as P
+    h = ct.libFDTD.FDTD_new()
+    code, msg = ct.last_error(h)
+    assert code == ct.FDTD_ERR_NODEVICE and "no CUDA device" in msg
+    opt, res = ct.SolveOptions(), ct.SolveResult()
+    opt.Tn = 10
+    assert ct.libFDTD.FDTD_solve_cw(h, ctypes.byref(opt), ctypes.byref(res)) == ct.FDTD_ERR_NODEVICE
+    ct.libFDTD.FDTD_delete(h)
+    with pytest.raises(ct.FDTDError):
+        P.make_solver(P.random_box(0))
+
+
+def test_argument_errors_are_reported():
+    from emopt_b200 import fdtd_ctypes as ct
+    h = ct.libFDTD.FDTD_new()
+    assert ct.libFDTD.FDTD_set_precision(h, 16) == ct.FDTD_ERR_ARG
+    assert "precision" in ct.last_error(h)[1]
+    assert ct.libFDTD.FDTD_set_kernel(h, 7) == ct.FDTD_ERR_ARG
+    ct.libFDTD.FDTD_delete(h)

@@ -1,0 +1,201 @@
+"""GPU parity tests: the CUDA library against the CPU oracle and the golden
+fixtures generated from the reference core.
+
+Tolerances: the per-call padded-layout path and the device-resident fp64 solve
+compute the reference's arithmetic in float64 with fused multiply-adds, so they
+agree with the oracle to rounding (relative L2 <= 1e-11 on the small blocks,
+<= 1e-9 on the full-size waveguide -- the tolerance the fp64 path is held to).
+The fp32 storage form is held to a relative L2 <= 1e-4 against the fp64 oracle.
+"""
+import numpy as np
+import pytest
+
+from emopt_b200 import problems as P
+from helpers import golden, input_digest, oracle_for, oracle_lib, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+BOX_KW = {
+    "pec": dict(seed=1, bc="000"),
+    "sym_EH0": dict(seed=2, bc="EH0"),
+    "sym_HEH": dict(seed=3, bc="HEH"),
+    "sym_0EE": dict(seed=4, bc="0EE"),
+    "lossy": dict(seed=5, complex_eps=True, bc="0H0"),
+    "mu_two_src": dict(seed=6, mu_random=True, n_sources=2, bc="E00"),
+    "wide_pml": dict(seed=7, shape=(12, 10, 16), w_pml=(5, 5, 4, 4, 5, 5), bc="000"),
+    "no_pml": dict(seed=8, shape=(8, 9, 10), w_pml=(0, 0, 0, 0, 0, 0), bc="H0E"),
+}
+
+
+def cuda_lib_path():
+    from emopt_b200 import fdtd_ctypes as ct
+    return ct.so_path
+
+
+def solve_gpu(p, precision="fp64", kernel="fused"):
+    sim = P.make_solver(p, precision=precision, kernel=kernel)
+    info = sim._solve([sim._Ex_fwd_t0, sim._Ey_fwd_t0, sim._Ez_fwd_t0, sim._Hx_fwd_t0,
+                       sim._Hy_fwd_t0, sim._Hz_fwd_t0],
+                      [sim._Ex_fwd_t1, sim._Ey_fwd_t1, sim._Ez_fwd_t1, sim._Hx_fwd_t1,
+                       sim._Hy_fwd_t1, sim._Hz_fwd_t1], sim._sources)
+    F = np.stack([sim._raw(c, False) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")])
+    return F, info, sim
+
+
+# ------------------------------------------------ per-call reference ABI
+@pytest.mark.parametrize("name", list(BOX_KW))
+def test_abi_per_call_path_matches_golden(name):
+    """The reference driver loop run unchanged over the CUDA library's per-call
+    entry points (update_H/E, capture, 3T extraction, in-place source conversion)."""
+    g = golden(f"box_{name}.npz")
+    p = P.random_box(**BOX_KW[name])
+    assert input_digest(p) == str(g["digest"])
+    r = oracle_for(p, lib=cuda_lib_path()).solve(fixed_steps=p.fixed_steps)
+    assert r["steps"] == int(g["steps"])
+    assert rel_l2(np.stack(r["fields"]), g["fields"]) < 1e-11
+
+
+def test_abi_per_call_chunked_local_grid():
+    """Chunks set with FDTD_set_local_grid (the reference's MPI decomposition),
+    ghost planes exchanged between per-chunk handles."""
+    p = P.random_box(41, shape=(12, 9, 11), bc="HE0", n_sources=2, fixed_steps=100)
+    a = oracle_for(p, oracle_lib()).solve(fixed_steps=p.fixed_steps)
+    b = oracle_for(p, lib=cuda_lib_path()).run_fixed_slabs(p.fixed_steps, 3)
+    assert rel_l2(np.stack(b["fields"]), np.stack(a["fields"])) < 1e-11
+
+
+def test_abi_per_call_field_arrays_match_oracle_each_step():
+    """After every half step the caller's padded field arrays (ghosts included)
+    equal the oracle's."""
+    from oracle import driver
+    p = P.random_box(42, bc="EH0", fixed_steps=30)
+    sims = [oracle_for(p, oracle_lib()), oracle_for(p, lib=cuda_lib_path())]
+    states = []
+    for s in sims:
+        lib = s.lib
+        I, J, K = s.Nz, s.Ny, s.Nx
+        npad = (I + 2) * (J + 2) * (K + 2)
+        E = [np.zeros(npad) for _ in range(3)]
+        H = [np.zeros(npad) for _ in range(3)]
+        mats = [a.ravel() for a in s.eps + s.mu]
+        t0 = [np.zeros(I * J * K, dtype=np.complex128) for _ in range(6)]
+        t1 = [np.zeros(I * J * K, dtype=np.complex128) for _ in range(6)]
+        h = lib.FDTD_new()
+        s._configure(h, 0, 0, 0, K, J, I, E, H, mats, t0, t1)
+        keep = []
+        s._add_sources(h, 0, I, keep)
+        lib.FDTD_reset_pml(h)
+        states.append((lib, h, E, H, keep, mats, t0, t1))
+    dt = sims[0].dt
+    for n in range(20):
+        for lib, h, E, H, *_ in states:
+            lib.FDTD_update_H(h, n, n * dt)
+        for a, b in zip(states[0][3], states[1][3]):
+            assert rel_l2(b, a) < 1e-12
+        for lib, h, E, H, *_ in states:
+            lib.FDTD_update_E(h, n, (n + 0.5) * dt)
+        for a, b in zip(states[0][2] + states[0][3], states[1][2] + states[1][3]):
+            assert rel_l2(b, a) < 1e-12
+    for lib, h, *_ in states:
+        lib.FDTD_capture_t0_fields(h)
+        lib.FDTD_calc_complex_fields_2T(h, 0.3, 20 * dt)
+    for a, b in zip(states[0][6], states[1][6]):
+        assert rel_l2(b, a) < 1e-12
+    # the source arrays were rewritten in place as (amplitude, -phase)
+    for ka, kb in zip(states[0][4], states[1][4]):
+        for a, b in zip(ka, kb):
+            assert rel_l2(b, a) < 1e-14
+    del driver
+
+
+# ------------------------------------------------ device-resident solve
+@pytest.mark.parametrize("kernel", ["fused", "unfused"])
+@pytest.mark.parametrize("name", list(BOX_KW))
+def test_solve_cw_fp64_matches_golden(name, kernel):
+    g = golden(f"box_{name}.npz")
+    p = P.random_box(**BOX_KW[name])
+    F, info, _ = solve_gpu(p, "fp64", kernel)
+    assert info["steps"] == int(g["steps"])
+    assert rel_l2(F, g["fields"]) < 1e-11
+
+
+@pytest.mark.parametrize("kernel", ["fused", "unfused"])
+def test_solve_cw_fp64_converging_step_count(kernel):
+    """Run to rtol = 1e-6: the step count is bit-for-bit the reference's."""
+    g = golden("box_converge.npz")
+    p = P.random_box(seed=11, shape=(10, 12, 15), fixed_steps=None, rtol=1e-6)
+    p.Nmax = 40000
+    F, info, _ = solve_gpu(p, "fp64", kernel)
+    assert info["n_main"] == int(g["n_main"]) and info["steps"] == int(g["steps"])
+    assert info["nprobes"] == len(g["history"])
+    assert info["A_change"] == pytest.approx(g["history"][-1][1], rel=1e-6)
+    assert rel_l2(F, g["fields"]) < 1e-9
+
+
+def test_solve_cw_waveguide_fp64_fingerprint():
+    """Full-size 101 x 76 x 65 waveguide, 4000 + 2 Tn steps, fp64: within 1e-9 of
+    the reference fingerprint."""
+    g = golden("waveguide.npz")
+    p = P.waveguide()
+    F, info, _ = solve_gpu(p, "fp64", "fused")
+    assert info["steps"] == int(g["steps"])
+    idx = g["idx"]
+    s = F[idx[:, 0], idx[:, 1], idx[:, 2], idx[:, 3]]
+    assert rel_l2(s, g["samples"]) < 1e-9
+    norms = np.sqrt(np.sum(np.abs(F) ** 2, axis=(1, 2, 3)))
+    assert rel_l2(norms, g["norms"]) < 1e-9
+
+
+def test_solve_cw_waveguide_full_field_vs_oracle():
+    """Whole complex field of the full-size waveguide against the oracle run on
+    the host cores (z-slab threads; bit-identical to one rank)."""
+    import os
+    p = P.waveguide()
+    ref = np.stack(oracle_for(p, oracle_lib()).run_fixed_slabs(p.fixed_steps,
+                                                               min(32, os.cpu_count() or 1))["fields"])
+    F64, _, _ = solve_gpu(p, "fp64", "fused")
+    assert rel_l2(F64, ref) < 1e-9
+    F64u, _, _ = solve_gpu(p, "fp64", "unfused")
+    assert rel_l2(F64u, ref) < 1e-9
+    F32, _, _ = solve_gpu(p, "fp32", "fused")
+    err32 = rel_l2(F32, ref)
+    print("waveguide fp32 relative L2 vs fp64 oracle: %.3e" % err32)
+    assert err32 < 1e-4
+
+
+@pytest.mark.parametrize("kernel", ["fused", "unfused"])
+def test_fp32_box_error(kernel):
+    g = golden("box_converge.npz")
+    p = P.random_box(seed=11, shape=(10, 12, 15), fixed_steps=None, rtol=1e-6)
+    p.Nmax = 40000
+    F, info, _ = solve_gpu(p, "fp32", kernel)
+    assert rel_l2(F, g["fields"]) < 1e-4
+
+
+def test_materials_unchanged_reuses_coefficients():
+    p = P.random_box(seed=1, bc="000")
+    g = golden("box_pec.npz")
+    sim = P.make_solver(p)
+    t0 = [sim._Ex_fwd_t0, sim._Ey_fwd_t0, sim._Ez_fwd_t0, sim._Hx_fwd_t0, sim._Hy_fwd_t0,
+          sim._Hz_fwd_t0]
+    t1 = [sim._Ex_fwd_t1, sim._Ey_fwd_t1, sim._Ez_fwd_t1, sim._Hx_fwd_t1, sim._Hy_fwd_t1,
+          sim._Hz_fwd_t1]
+    for _ in range(2):   # second solve reuses the device coefficients
+        sim._solve(t0, t1, sim._sources)
+        F = np.stack([sim._raw(c, False) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")])
+        assert rel_l2(F, g["fields"]) < 1e-11
+    assert sim._materials_dirty is False
+
+
+def test_source_outside_grid_is_an_error():
+    import ctypes
+    from emopt_b200 import fdtd_ctypes as ct
+    p = P.random_box(seed=1)
+    sim = P.make_solver(p)
+    h = sim._libfdtd
+    z = np.zeros(4, dtype=np.complex128)
+    ct.libFDTD.FDTD_add_source(h, z, z, z, z, z, z, p.shape[0] - 1, 0, 0, 2, 2, 1, False)
+    opt, res = ct.SolveOptions(), ct.SolveResult()
+    opt.Tn, opt.Nmax, opt.rtol, opt.nconv = 10, 5.0, 1e-6, 0
+    rc = ct.libFDTD.FDTD_solve_cw(h, ctypes.byref(opt), ctypes.byref(res))
+    assert rc == ct.FDTD_ERR_ARG and "outside the grid" in ct.last_error(h)[1]
