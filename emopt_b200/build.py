@@ -18,8 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "FDTD.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["fdtd_abi.cu", "step_kernels.cu", "fused_kernels.cu", "aux_kernels.cu",
-           "legacy_kernels.cu"]
+SOURCES = ["fdtd_abi.cu", "step_kernels.cu", "fused_kernels.cu", "tma_kernels.cu",
+           "aux_kernels.cu", "legacy_kernels.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]

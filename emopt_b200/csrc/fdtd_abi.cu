@@ -72,7 +72,9 @@ struct Resident {
     DevBuf stage;            // complex128 staging (one component)
     std::vector<DevBuf> src_ap;    // per source: 6 comps of amp/phase (complex128)
     std::vector<DevBuf> src_coef;  // per source: 6 comps of (a_c, a_s)
-    DevBuf steptab, stepbase, flag;
+    DevBuf steptab, stepbase, flag, err;
+    fdtdb::StepMaps maps[2];
+    bool maps_valid = false;
     DevBuf pwin, pA, pphi, ptimes, pout, pmap;
 
     void release_all() {
@@ -85,7 +87,8 @@ struct Resident {
         for (auto& b : src_ap) b.release();
         for (auto& b : src_coef) b.release();
         src_ap.clear(); src_coef.clear();
-        steptab.release(); stepbase.release(); flag.release();
+        steptab.release(); stepbase.release(); flag.release(); err.release();
+        maps_valid = false;
         pwin.release(); pA.release(); pphi.release(); ptimes.release(); pout.release(); pmap.release();
         coeffs_valid = false;
         Nx = Ny = Nz = px = 0;
@@ -123,6 +126,7 @@ struct FDTDHandle {
     std::string message;
     int precision = 64;
     int kernel = 0;
+    int zchunk = 0;   // planes per CTA of the TMA kernel (0: automatic)
 
     // ---- padded-layout device mirrors for the per-call entry points
     DevBuf lE[3], lH[3], leps[3], lmu[3];
@@ -713,7 +717,7 @@ int FDTD_set_precision(FDTDHandle* h, int bits) {
 }
 
 int FDTD_set_kernel(FDTDHandle* h, int which) {
-    if (which != 0 && which != 1) return h->fail(FDTD_ERR_ARG, "kernel must be 0 or 1");
+    if (which < 0 || which > 2) return h->fail(FDTD_ERR_ARG, "kernel must be 0, 1 or 2");
     h->kernel = which;
     return FDTD_OK;
 }
@@ -726,6 +730,59 @@ namespace {
 template <typename T> Resident<T>& resident(FDTDHandle* h);
 template <> Resident<float>& resident<float>(FDTDHandle* h) { return h->r32; }
 template <> Resident<double>& resident<double>(FDTDHandle* h) { return h->r64; }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// 3D map over one pitched [Nz][Ny][px] component with box (bx, by, 1).
+template <typename T>
+bool encode_plane_map(CUtensorMap* m, void* base, int px, int Ny, int Nz, int bx, int by) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)px, (cuuint64_t)Ny, (cuuint64_t)Nz};
+    cuuint64_t strides[2] = {(cuuint64_t)px * sizeof(T), (cuuint64_t)px * Ny * sizeof(T)};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUtensorMapDataType dt =
+        sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    return fn(m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps for reading set 0 and set 1 (E, H) and the E coefficients.
+template <typename T>
+bool build_maps(FDTDHandle* h, Resident<T>& r) {
+    int TY = fdtdb::tma_tile_rows();
+    for (int s = 0; s < 2; s++)
+        for (int c = 0; c < 3; c++) {
+            if (!encode_plane_map<T>(&r.maps[s].E[c], r.F[s][c].p, r.px, h->Ny, h->Nz, 40, TY + 2))
+                return false;
+            if (!encode_plane_map<T>(&r.maps[s].H[c], r.F[s][3 + c].p, r.px, h->Ny, h->Nz, 36, TY + 1))
+                return false;
+            if (!encode_plane_map<T>(&r.maps[s].B[c], r.bE[c].p, r.px, h->Ny, h->Nz, 32, TY))
+                return false;
+        }
+    return true;
+}
 
 // Allocates the resident arrays for the current grid and PML widths.
 template <typename T>
@@ -748,6 +805,7 @@ int alloc_resident(FDTDHandle* h, Resident<T>& r, bool two_sets) {
         for (int c = 0; c < 6; c++) CK(r.snap[s][c].ensure(sizeof(T) * cells));
     CK(r.stepbase.ensure(sizeof(long long)));
     CK(r.flag.ensure(sizeof(int) * 4));
+    CK(r.err.ensure(sizeof(int) * 4));
     return FDTD_OK;
 }
 
@@ -920,10 +978,15 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     bool periodic = false;
     for (int a = 0; a < 3; a++)
         if (h->bc[a] != '0' && h->bc[a] != 'E' && h->bc[a] != 'H') periodic = true;
-    bool fused = h->kernel == 0 && !periodic;
+    bool fused = h->kernel != 1 && !periodic;
+    bool small_index = (long long)h->Nz * h->Ny * ((h->Nx + 31) / 32 * 32) < (1LL << 31) &&
+                       (long long)h->Nz * h->Ny * (h->w[0] + h->w[1]) < (1LL << 31);
+    bool tma = fused && h->kernel == 0 && small_index && encode_fn() != nullptr;
     int rc;
     CK(cudaEventRecord(h->ev[2], h->stream));
     if ((rc = alloc_resident<T>(h, r, fused)) != FDTD_OK) return rc;
+    if (tma && !build_maps<T>(h, r)) tma = false;
+    CK(cudaMemsetAsync(r.err.p, 0, sizeof(int), h->stream));
     if (!o->materials_unchanged || !r.coeffs_valid) {
         if ((rc = prepare_materials<T>(h, r)) != FDTD_OK) return rc;
         launches += 3 + 3 + 3;   // eps coefficients, uniform checks, mu coefficients (upper bound)
@@ -975,6 +1038,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     pd.nconv = nconv;
 
     long long* sb = dptr<long long>(r.stepbase);
+    int zchunk = h->zchunk > 0 ? h->zchunk : (h->Nz < 32 ? h->Nz : 32);
     fdtdb::GridView<T> g0 = make_view<T>(h, r, 0);
     fdtdb::GridView<T> g1 = fused ? make_view<T>(h, r, 1) : g0;
     T* f0[6];
@@ -987,10 +1051,15 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     auto cur_set = [&](long long steps) -> T* const* { return (fused && (steps & 1)) ? f1 : f0; };
     auto run = [&](long long n_first, long long count) -> int {
         fdtdb::launch_set_ll(sb, n_first, h->stream);
-        launches += 1 + count * (fused ? 1 : 2);
+        launches += 1 + count * ((fused || tma) ? 1 : 2);
         for (long long q = 0; q < count; q++) {
             long long n = n_first + q;
-            if (fused) {
+            if (tma) {
+                bool odd = n & 1;
+                CK(fdtdb::launch_step_tma<T>(r.maps[odd ? 1 : 0], odd ? g1 : g0, odd ? g0 : g1,
+                                             odd ? f0 : f1, src, sb, (int)q, zchunk,
+                                             dptr<int>(r.err), h->stream));
+            } else if (fused) {
                 bool odd = n & 1;
                 fdtdb::launch_step_fused<T>(odd ? g1 : g0, odd ? g0 : g1, odd ? f1 : f0,
                                             odd ? f0 : f1, src, sb, (int)q, h->stream);
@@ -1074,7 +1143,10 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
         }
     }
     CK(cudaEventRecord(h->ev[3], h->stream));
+    int kerr = 0;
+    CK(cudaMemcpyAsync(&kerr, r.err.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     if ((rc = h->sync_check("FDTD_solve_cw")) != FDTD_OK) return rc;
+    if (kerr) return h->fail(FDTD_ERR_CUDA, "a bounded wait in the step kernel gave up (code %d)", kerr);
     float ms_steps = 0, ms_total = 0;
     cudaEventElapsedTime(&ms_steps, h->ev[0], h->ev[1]);
     cudaEventElapsedTime(&ms_total, h->ev[2], h->ev[3]);

@@ -1,6 +1,8 @@
 // kernels.h -- host-side launch wrappers for the CUDA kernels.
 #pragma once
 
+#include <cuda.h>
+
 #include "grid.cuh"
 
 namespace fdtdb {
@@ -16,6 +18,23 @@ template <typename T>
 void launch_step_fused(const GridView<T>& ga, const GridView<T>& gb, T* const* fa, T* const* fb,
                        const SourceList<T>& src, const long long* step_base, int off,
                        cudaStream_t st);
+
+// TMA descriptors of one read set: E and H components (3D [Nz][Ny][px],
+// boxes 40 x (TY+2) and 36 x (TY+1)) and the E-update coefficients (32 x TY).
+struct StepMaps {
+    CUtensorMap E[3];
+    CUtensorMap H[3];
+    CUtensorMap B[3];
+};
+
+int tma_tile_rows();
+
+// Fused step with TMA-staged planes (tma_kernels.cu); *err is set when a
+// bounded wait gives up.
+template <typename T>
+cudaError_t launch_step_tma(const StepMaps& maps, const GridView<T>& ga, const GridView<T>& gb,
+                            T* const* fb, const SourceList<T>& src, const long long* step_base,
+                            int off, int zc, int* err, cudaStream_t st);
 
 // eps or mu (complex128, dense [Nz][Ny][Nx]) -> pitched update coefficients.
 // b = dt/eps.real, or for lossy media a = (er/dt - ei/2)/(er/dt + ei/2),

@@ -14,7 +14,8 @@ instead of MPI ranks:
   whole time loop of ``FDTD.__solve`` (``emopt/fdtd.py:994-1194``) on the
   device and returns the complex steady-state fields;
 * extra keyword arguments: ``precision`` (``'fp64'`` = reference arithmetic,
-  ``'fp32'`` = float32 storage), ``kernel`` (``'fused'`` or ``'unfused'``) and
+  ``'fp32'`` = float32 storage), ``kernel`` (``'fused'``, ``'unfused'`` or
+  ``'fused_plain'``) and
   ``device`` (CUDA device index).
 
 Materials are any objects with ``get_values(k1, k2, j1, j2, i1, i2, sx, sy, sz,
@@ -100,6 +101,10 @@ class MaxwellSolver:
 class FDTD(MaxwellSolver):
     """3D continuous-wave FDTD solver (drop-in for ``emopt.fdtd.FDTD``)."""
 
+    # time-stepping kernels of FDTD_solve_cw: fused with TMA-staged planes,
+    # separate H/E sweeps, fused with plain loads
+    KERNELS = {"fused": 0, "unfused": 1, "fused_plain": 2}
+
     def __init__(self, X, Y, Z, dx, dy, dz, wavelength, rtol=1e-6, nconv=None,
                  min_rindex=1.0, complex_eps=False, dist_method="auto",
                  precision="fp64", kernel="fused", device=None):
@@ -111,8 +116,8 @@ class FDTD(MaxwellSolver):
                             "emopt_b200.fdtd")
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32'")
-        if kernel not in ("fused", "unfused"):
-            raise ValueError("kernel must be 'fused' or 'unfused'")
+        if kernel not in self.KERNELS:
+            raise ValueError("kernel must be one of %s" % (sorted(self.KERNELS),))
         self._dx, self._dy, self._dz = dx, dy, dz
         prm = derive_parameters(X, Y, Z, dx, dy, dz, wavelength, min_rindex, nconv)
         Nx, Ny, Nz = prm["Nx"], prm["Ny"], prm["Nz"]
@@ -165,7 +170,7 @@ class FDTD(MaxwellSolver):
                                     self._mu_x, self._mu_y, self._mu_z)
         libFDTD.FDTD_set_complex_eps(h, complex_eps)
         libFDTD.FDTD_set_precision(h, 32 if precision == "fp32" else 64)
-        libFDTD.FDTD_set_kernel(h, 0 if kernel == "fused" else 1)
+        libFDTD.FDTD_set_kernel(h, self.KERNELS[kernel])
 
         # CPML defaults (emopt/fdtd.py:368-390)
         w_pml = 15
@@ -478,7 +483,7 @@ class FDTD(MaxwellSolver):
         self.last_solve = {"n_main": res.n_main, "steps": res.steps, "A_change": res.A_change,
                            "phi_change": res.phi_change, "nprobes": res.nprobes,
                            "device_ms": res.device_ms, "total_ms": res.total_ms,
-                           "status": status}
+                           "launches": res.launches, "status": status}
         return self.last_solve
 
     def solve_forward(self):

