@@ -49,7 +49,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--kernel", default="fused", choices=["fused", "unfused"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "scalar", "fused_plain", "fused_tma", "fused_warp", "vector"])
     ap.add_argument("--workload", default="mmi", choices=["mmi", "waveguide"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the fp64 comparison solve")

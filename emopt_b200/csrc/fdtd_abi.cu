@@ -126,7 +126,7 @@ struct FDTDHandle {
     std::string message;
     int precision = 64;
     int kernel = 0;
-    int zchunk = 0;   // planes per CTA of the TMA kernel (0: automatic)
+    int zchunk = 0;   // planes per CTA of the fused kernels (0: automatic)
 
     // ---- padded-layout device mirrors for the per-call entry points
     DevBuf lE[3], lH[3], leps[3], lmu[3];
@@ -710,6 +710,12 @@ int FDTD_set_device(FDTDHandle* h, int device) {
     return FDTD_OK;
 }
 
+int FDTD_set_zchunk(FDTDHandle* h, int planes) {
+    if (planes < 0) return h->fail(FDTD_ERR_ARG, "planes per CTA must be >= 0");
+    h->zchunk = planes;
+    return FDTD_OK;
+}
+
 int FDTD_set_precision(FDTDHandle* h, int bits) {
     if (bits != 32 && bits != 64) return h->fail(FDTD_ERR_ARG, "precision must be 32 or 64");
     h->precision = bits;
@@ -717,7 +723,7 @@ int FDTD_set_precision(FDTDHandle* h, int bits) {
 }
 
 int FDTD_set_kernel(FDTDHandle* h, int which) {
-    if (which < 0 || which > 2) return h->fail(FDTD_ERR_ARG, "kernel must be 0, 1 or 2");
+    if (which < 0 || which > 5) return h->fail(FDTD_ERR_ARG, "kernel must be in 0..5");
     h->kernel = which;
     return FDTD_OK;
 }
@@ -978,10 +984,17 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     bool periodic = false;
     for (int a = 0; a < 3; a++)
         if (h->bc[a] != '0' && h->bc[a] != 'E' && h->bc[a] != 'H') periodic = true;
-    bool fused = h->kernel != 1 && !periodic;
     bool small_index = (long long)h->Nz * h->Ny * ((h->Nx + 31) / 32 * 32) < (1LL << 31) &&
                        (long long)h->Nz * h->Ny * (h->w[0] + h->w[1]) < (1LL << 31);
-    bool tma = fused && h->kernel == 0 && small_index && encode_fn() != nullptr;
+    // kernel ids: 0 auto, 1 scalar H/E pair, 2 fused CTA tiles (plain loads),
+    // 3 fused CTA tiles (TMA), 4 fused warp tiles, 5 vector H/E pair
+    int kid = h->kernel == 0 ? 5 : h->kernel;
+    if (periodic || !small_index) kid = 1;
+    if (kid == 3 && encode_fn() == nullptr) kid = 5;
+    bool vec = kid == 5;
+    bool warp = kid == 4;
+    bool tma = kid == 3;
+    bool fused = kid == 2 || kid == 3 || kid == 4;
     int rc;
     CK(cudaEventRecord(h->ev[2], h->stream));
     if ((rc = alloc_resident<T>(h, r, fused)) != FDTD_OK) return rc;
@@ -1038,7 +1051,10 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     pd.nconv = nconv;
 
     long long* sb = dptr<long long>(r.stepbase);
-    int zchunk = h->zchunk > 0 ? h->zchunk : (h->Nz < 32 ? h->Nz : 32);
+    int zchunk = h->zchunk > 0 ? h->zchunk : (h->Nz < 32 ? h->Nz : 32);   // TMA kernel
+    int wz = h->zchunk;
+    if (warp && wz <= 0) CK(fdtdb::warp_zchunk<T>(h->Nx, h->Ny, h->Nz, &wz, nullptr));
+    if (tma) wz = zchunk;
     fdtdb::GridView<T> g0 = make_view<T>(h, r, 0);
     fdtdb::GridView<T> g1 = fused ? make_view<T>(h, r, 1) : g0;
     T* f0[6];
@@ -1051,10 +1067,14 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     auto cur_set = [&](long long steps) -> T* const* { return (fused && (steps & 1)) ? f1 : f0; };
     auto run = [&](long long n_first, long long count) -> int {
         fdtdb::launch_set_ll(sb, n_first, h->stream);
-        launches += 1 + count * ((fused || tma) ? 1 : 2);
+        launches += 1 + count * (fused ? 1 : 2);
         for (long long q = 0; q < count; q++) {
             long long n = n_first + q;
-            if (tma) {
+            if (warp) {
+                bool odd = n & 1;
+                CK(fdtdb::launch_step_warp<T>(odd ? g1 : g0, odd ? g0 : g1, odd ? f1 : f0,
+                                              odd ? f0 : f1, src, sb, (int)q, wz, h->stream));
+            } else if (tma) {
                 bool odd = n & 1;
                 CK(fdtdb::launch_step_tma<T>(r.maps[odd ? 1 : 0], odd ? g1 : g0, odd ? g0 : g1,
                                              odd ? f0 : f1, src, sb, (int)q, zchunk,
@@ -1063,6 +1083,8 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
                 bool odd = n & 1;
                 fdtdb::launch_step_fused<T>(odd ? g1 : g0, odd ? g0 : g1, odd ? f1 : f0,
                                             odd ? f0 : f1, src, sb, (int)q, h->stream);
+            } else if (vec) {
+                CK(fdtdb::launch_step_vec<T>(g0, f0, src, sb, (int)q, h->stream));
             } else {
                 fdtdb::launch_step_unfused<T>(g0, f0, src, sb, (int)q, h->stream);
             }
@@ -1158,6 +1180,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     res->device_ms = ms_steps;
     res->total_ms = ms_total;
     res->launches = launches;
+    res->zchunk = (warp || tma) ? wz : 0;
     res->status = FDTD_OK;
     if (!fixed && not_converged()) {
         bool bad = std::isnan(Ach) || std::isinf(Ach) || std::isnan(Pch) || std::isinf(Pch);

@@ -12,6 +12,12 @@ template <typename T>
 void launch_step_unfused(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
                          const long long* step_base, int off, cudaStream_t st);
 
+// In-place H and E half steps, one 16-byte vector of x cells per thread
+// (vec_kernels.cu).  Requires non-periodic boundaries.
+template <typename T>
+cudaError_t launch_step_vec(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
+                            const long long* step_base, int off, cudaStream_t st);
+
 // One fused time step reading set A (ga's CPML state, fields fa) and writing
 // set B (gb's CPML state, fields fb).  Requires non-periodic boundaries.
 template <typename T>
@@ -28,6 +34,17 @@ struct StepMaps {
 };
 
 int tma_tile_rows();
+
+// Planes per CTA for the warp-tile kernel: balances the last wave of CTAs
+// (occupancy x SM count slots) against the per-chunk prologue.
+template <typename T>
+cudaError_t warp_zchunk(int Nx, int Ny, int Nz, int* zc, int* slots);
+
+// Fused step on warp-independent register tiles (warp_kernels.cu), zc planes per CTA.
+template <typename T>
+cudaError_t launch_step_warp(const GridView<T>& ga, const GridView<T>& gb, T* const* fa,
+                             T* const* fb, const SourceList<T>& src, const long long* step_base,
+                             int off, int zc, cudaStream_t st);
 
 // Fused step with TMA-staged planes (tma_kernels.cu); *err is set when a
 // bounded wait gives up.

@@ -14,8 +14,8 @@ instead of MPI ranks:
   whole time loop of ``FDTD.__solve`` (``emopt/fdtd.py:994-1194``) on the
   device and returns the complex steady-state fields;
 * extra keyword arguments: ``precision`` (``'fp64'`` = reference arithmetic,
-  ``'fp32'`` = float32 storage), ``kernel`` (``'fused'``, ``'unfused'`` or
-  ``'fused_plain'``) and
+  ``'fp32'`` = float32 storage), ``kernel`` (one of ``FDTD.KERNELS``,
+  default ``'auto'``) and
   ``device`` (CUDA device index).
 
 Materials are any objects with ``get_values(k1, k2, j1, j2, i1, i2, sx, sy, sz,
@@ -101,13 +101,13 @@ class MaxwellSolver:
 class FDTD(MaxwellSolver):
     """3D continuous-wave FDTD solver (drop-in for ``emopt.fdtd.FDTD``)."""
 
-    # time-stepping kernels of FDTD_solve_cw: fused with TMA-staged planes,
-    # separate H/E sweeps, fused with plain loads
-    KERNELS = {"fused": 0, "unfused": 1, "fused_plain": 2}
+    # time-stepping kernels of FDTD_solve_cw (include/emopt_fdtd.h, FDTD_set_kernel)
+    KERNELS = {"auto": 0, "scalar": 1, "fused_plain": 2, "fused_tma": 3, "fused_warp": 4,
+               "vector": 5}
 
     def __init__(self, X, Y, Z, dx, dy, dz, wavelength, rtol=1e-6, nconv=None,
                  min_rindex=1.0, complex_eps=False, dist_method="auto",
-                 precision="fp64", kernel="fused", device=None):
+                 precision="fp64", kernel="auto", device=None):
         super().__init__(3)
         if nconv is None:
             nconv = 10
@@ -483,7 +483,7 @@ class FDTD(MaxwellSolver):
         self.last_solve = {"n_main": res.n_main, "steps": res.steps, "A_change": res.A_change,
                            "phi_change": res.phi_change, "nprobes": res.nprobes,
                            "device_ms": res.device_ms, "total_ms": res.total_ms,
-                           "launches": res.launches, "status": status}
+                           "launches": res.launches, "zchunk": res.zchunk, "status": status}
         return self.last_solve
 
     def solve_forward(self):

@@ -118,7 +118,8 @@ class SolveOptions(Structure):
 class SolveResult(Structure):
     _fields_ = [("n_main", c_longlong), ("steps", c_longlong), ("A_change", c_double),
                 ("phi_change", c_double), ("nprobes", c_longlong), ("device_ms", c_double),
-                ("total_ms", c_double), ("launches", c_longlong), ("status", c_int)]
+                ("total_ms", c_double), ("launches", c_longlong), ("zchunk", c_int),
+                ("status", c_int)]
 
 
 FDTD_OK, FDTD_ERR_CUDA, FDTD_ERR_ARG, FDTD_ERR_NODEVICE, FDTD_NMAX, FDTD_NONFINITE = range(6)
@@ -129,6 +130,8 @@ libFDTD.FDTD_last_error.argtypes = [c_void_p, c_char_p, c_int]
 libFDTD.FDTD_last_error.restype = c_int
 libFDTD.FDTD_set_device.argtypes = [c_void_p, c_int]
 libFDTD.FDTD_set_device.restype = c_int
+libFDTD.FDTD_set_zchunk.argtypes = [c_void_p, c_int]
+libFDTD.FDTD_set_zchunk.restype = c_int
 libFDTD.FDTD_set_precision.argtypes = [c_void_p, c_int]
 libFDTD.FDTD_set_precision.restype = c_int
 libFDTD.FDTD_set_kernel.argtypes = [c_void_p, c_int]
@@ -136,8 +139,8 @@ libFDTD.FDTD_set_kernel.restype = c_int
 libFDTD.FDTD_solve_cw.argtypes = [c_void_p, POINTER(SolveOptions), POINTER(SolveResult)]
 libFDTD.FDTD_solve_cw.restype = c_int
 
-ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_precision",
-                 "FDTD_set_kernel", "FDTD_solve_cw")
+ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_zchunk",
+                 "FDTD_set_precision", "FDTD_set_kernel", "FDTD_solve_cw")
 
 
 class FDTDError(RuntimeError):

@@ -197,7 +197,7 @@ def random_box(seed: int, shape=(9, 11, 14), d=0.04, w_pml=(3, 4, 3, 2, 3, 4), b
     return p
 
 
-def make_solver(p: Problem, precision: str = "fp64", kernel: str = "fused", device=None):
+def make_solver(p: Problem, precision: str = "fp64", kernel: str = "auto", device=None):
     """Configure an ``emopt_b200.fdtd.FDTD`` for problem ``p`` (sources added, not solved)."""
     from .fdtd import FDTD
     from .misc import DomainCoordinates

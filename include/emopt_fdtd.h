@@ -111,14 +111,20 @@ int FDTD_last_error(FDTDHandle *h, char *buf, int buflen);
  * device).  Must precede the first call that touches the device. */
 int FDTD_set_device(FDTDHandle *h, int device);
 
+/* Planes per CTA of the fused time-step kernels (0 = chosen from the
+ * occupancy, the default).  A tuning knob; results do not depend on it. */
+int FDTD_set_zchunk(FDTDHandle *h, int planes);
+
 /* Storage/arithmetic precision of FDTD_solve_cw: 64 (default, the reference's
  * float64) or 32 (fields, coefficients and CPML state in float32; the
  * steady-state fit, probes and outputs stay float64).  Returns a status. */
 int FDTD_set_precision(FDTDHandle *h, int bits);
 
-/* Time-stepping kernel of FDTD_solve_cw: 0 = fused one-launch-per-step kernel
- * with TMA-staged planes (default), 1 = separate H and E kernels, 2 = fused
- * kernel with plain loads.  Periodic boundaries always use 1. */
+/* Time-stepping kernel of FDTD_solve_cw: 0 = automatic (default), 1 = H and
+ * E kernels with one cell per thread, 2 = fused CTA-tile kernel with plain
+ * loads, 3 = fused CTA-tile kernel with TMA-staged planes, 4 = fused kernel on
+ * warp-independent register tiles, 5 = H and E kernels with one 16-byte
+ * vector of x cells per thread.  Periodic boundaries always use 1. */
 int FDTD_set_kernel(FDTDHandle *h, int which);
 
 typedef struct {
@@ -141,6 +147,7 @@ typedef struct {
     double device_ms;          /* device time of all time steps (CUDA events) */
     double total_ms;           /* device time of the whole call incl. transfers */
     long long launches;        /* kernels this call launched */
+    int zchunk;                /* planes per CTA used by the fused kernel (0: not fused) */
     int status;                /* FDTD_OK, FDTD_NMAX or FDTD_NONFINITE */
 } FDTDSolveResult;
 

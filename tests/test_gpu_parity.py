@@ -32,7 +32,7 @@ def cuda_lib_path():
     return ct.so_path
 
 
-def solve_gpu(p, precision="fp64", kernel="fused"):
+def solve_gpu(p, precision="fp64", kernel="auto"):
     sim = P.make_solver(p, precision=precision, kernel=kernel)
     info = sim._solve([sim._Ex_fwd_t0, sim._Ey_fwd_t0, sim._Ez_fwd_t0, sim._Hx_fwd_t0,
                        sim._Hy_fwd_t0, sim._Hz_fwd_t0],
@@ -115,7 +115,7 @@ def test_abi_per_call_field_arrays_match_oracle_each_step():
 
 
 # ------------------------------------------------ device-resident solve
-@pytest.mark.parametrize("kernel", ["fused", "unfused", "fused_plain"])
+@pytest.mark.parametrize("kernel", ["vector", "scalar", "fused_plain", "fused_tma", "fused_warp"])
 @pytest.mark.parametrize("name", list(BOX_KW))
 def test_solve_cw_fp64_matches_golden(name, kernel):
     g = golden(f"box_{name}.npz")
@@ -125,7 +125,7 @@ def test_solve_cw_fp64_matches_golden(name, kernel):
     assert rel_l2(F, g["fields"]) < 1e-11
 
 
-@pytest.mark.parametrize("kernel", ["fused", "unfused", "fused_plain"])
+@pytest.mark.parametrize("kernel", ["vector", "scalar", "fused_plain", "fused_tma", "fused_warp"])
 def test_solve_cw_fp64_converging_step_count(kernel):
     """Run to rtol = 1e-6: the step count is bit-for-bit the reference's."""
     g = golden("box_converge.npz")
@@ -143,7 +143,7 @@ def test_solve_cw_waveguide_fp64_fingerprint():
     the reference fingerprint."""
     g = golden("waveguide.npz")
     p = P.waveguide()
-    F, info, _ = solve_gpu(p, "fp64", "fused")
+    F, info, _ = solve_gpu(p, "fp64", "auto")
     assert info["steps"] == int(g["steps"])
     idx = g["idx"]
     s = F[idx[:, 0], idx[:, 1], idx[:, 2], idx[:, 3]]
@@ -159,19 +159,16 @@ def test_solve_cw_waveguide_full_field_vs_oracle():
     p = P.waveguide()
     ref = np.stack(oracle_for(p, oracle_lib()).run_fixed_slabs(p.fixed_steps,
                                                                min(32, os.cpu_count() or 1))["fields"])
-    F64, _, _ = solve_gpu(p, "fp64", "fused")
-    assert rel_l2(F64, ref) < 1e-9
-    F64u, _, _ = solve_gpu(p, "fp64", "unfused")
-    assert rel_l2(F64u, ref) < 1e-9
-    F64p, _, _ = solve_gpu(p, "fp64", "fused_plain")
-    assert rel_l2(F64p, ref) < 1e-9
-    F32, _, _ = solve_gpu(p, "fp32", "fused")
+    for kern in ("vector", "scalar", "fused_plain", "fused_tma", "fused_warp"):
+        F64, _, _ = solve_gpu(p, "fp64", kern)
+        assert rel_l2(F64, ref) < 1e-9, kern
+    F32, _, _ = solve_gpu(p, "fp32", "auto")
     err32 = rel_l2(F32, ref)
     print("waveguide fp32 relative L2 vs fp64 oracle: %.3e" % err32)
     assert err32 < 1e-4
 
 
-@pytest.mark.parametrize("kernel", ["fused", "unfused"])
+@pytest.mark.parametrize("kernel", ["vector", "scalar", "fused_tma", "fused_warp"])
 def test_fp32_box_error(kernel):
     g = golden("box_converge.npz")
     p = P.random_box(seed=11, shape=(10, 12, 15), fixed_steps=None, rtol=1e-6)
