@@ -903,6 +903,11 @@ int prepare_sources(FDTDHandle* h, Resident<T>& r, fdtdb::SourceList<T>& list) {
         for (int c = 0; c < 6; c++) {
             d.comp[c] = nullptr;
             if (!hs.comp[c] || n <= 0) continue;
+            // a component that is zero everywhere adds nothing: leave it out so
+            // the half step it would drive skips the source test entirely
+            bool any = false;
+            for (long long q = 0; q < n && !any; q++) any = hs.comp[c][q].real != 0.0;
+            if (!any) continue;
             DevBuf& ap = r.src_ap[6 * s + c];
             DevBuf& co = r.src_coef[6 * s + c];
             CK(ap.ensure(sizeof(c128) * n));

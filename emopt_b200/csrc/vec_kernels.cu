@@ -1,4 +1,4 @@
-// vec_kernels.cu -- H and E half-steps, one 16-byte vector of x cells per thread.
+// vec_kernels.cu -- H and E half-steps, one vector of x cells per thread.
 //
 // The same in-place update as k_update_H / k_update_E (src/fdtd.cpp:121-367
 // and :369-755), restructured for throughput: a thread owns V = 2 consecutive
@@ -52,15 +52,17 @@ __device__ __forceinline__ void vstore(T* p, const T (&d)[V16<T>::N]) {
     *reinterpret_cast<typename V16<T>::type*>(p) = v;
 }
 
-// Does any source box touch rows [j0, j1), columns [k0, k1) of plane i?
+// Does a source box with a non-zero component among comp_base..comp_base+2
+// touch rows [j0, j1), columns [k0, k1) of plane i?
 template <typename T>
-__device__ __forceinline__ bool sources_touch(const SourceList<T>& src, int i, int j0, int j1,
-                                              int k0, int k1) {
+__device__ __forceinline__ bool sources_touch(const SourceList<T>& src, int comp_base, int i,
+                                              int j0, int j1, int k0, int k1) {
     bool hit = false;
     for (int q = 0; q < src.n; q++) {
         const DevSource<T>& s = src.s[q];
-        hit |= i >= s.i0 && i < s.i0 + s.I && s.j0 < j1 && s.j0 + s.J > j0 && s.k0 < k1 &&
-               s.k0 + s.K > k0;
+        const bool drives = s.comp[comp_base] || s.comp[comp_base + 1] || s.comp[comp_base + 2];
+        hit |= drives && i >= s.i0 && i < s.i0 + s.I && s.j0 < j1 && s.j0 + s.J > j0 &&
+               s.k0 < k1 && s.k0 + s.K > k0;
     }
     return hit;
 }
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(256) k_update_H_vec(GridView<T> g, Fields<T> f
     T mx[V], my[V], mz[V];
     const bool mu_arr = g.bHarr[0] != nullptr;
     if (mu_arr && act) { vload<T>(mx, g.bHarr[0] + p); vload<T>(my, g.bHarr[1] + p); vload<T>(mz, g.bHarr[2] + p); }
-    const bool srcb = src.n && sources_touch<T>(src, i, blockIdx.y * 8, blockIdx.y * 8 + 8,
+    const bool srcb = src.n && sources_touch<T>(src, 3, i, blockIdx.y * 8, blockIdx.y * 8 + 8,
                                                 blockIdx.x * 32 * V, (blockIdx.x + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_base + off];
@@ -249,7 +251,7 @@ __global__ void __launch_bounds__(256) k_update_E_vec(GridView<T> g, Fields<T> f
             px2[e] = ld(PX.psi[2] + s); px3[e] = ld(PX.psi[3] + s);
         }
     }
-    const bool srcb = src.n && sources_touch<T>(src, i, blockIdx.y * 8, blockIdx.y * 8 + 8,
+    const bool srcb = src.n && sources_touch<T>(src, 0, i, blockIdx.y * 8, blockIdx.y * 8 + 8,
                                                 blockIdx.x * 32 * V, (blockIdx.x + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_base + off];
