@@ -138,9 +138,15 @@ libFDTD.FDTD_set_kernel.argtypes = [c_void_p, c_int]
 libFDTD.FDTD_set_kernel.restype = c_int
 libFDTD.FDTD_solve_cw.argtypes = [c_void_p, POINTER(SolveOptions), POINTER(SolveResult)]
 libFDTD.FDTD_solve_cw.restype = c_int
+libFDTD.FDTD_amp_phase_noalloc.argtypes = [c_int, c_void_p,
+                                           ndpointer(np.complex128, flags="C_CONTIGUOUS"),
+                                           c_longlong, c_char_p, c_int]
+libFDTD.FDTD_amp_phase_noalloc.restype = c_int
+NOALLOC_MAX_VALUES = 524288
 
 ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_zchunk",
-                 "FDTD_set_precision", "FDTD_set_kernel", "FDTD_solve_cw")
+                 "FDTD_set_precision", "FDTD_set_kernel", "FDTD_solve_cw",
+                 "FDTD_amp_phase_noalloc")
 
 
 class FDTDError(RuntimeError):

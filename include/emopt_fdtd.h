@@ -158,6 +158,30 @@ typedef struct {
  * complex steady-state fields into the t0 arrays.  Returns a status. */
 int FDTD_solve_cw(FDTDHandle *h, const FDTDSolveOptions *opt, FDTDSolveResult *res);
 
+/* Largest n accepted by FDTD_amp_phase_noalloc: 524288 complex128 values, the
+ * 8 MiB device array it stages through. */
+#define FDTD_NOALLOC_MAX_VALUES 524288
+
+/* No counterpart in the reference.  Rewrites the n complex values of the host
+ * array a in place as (|a|, -atan2(im, re)) -- the conversion FDTD_add_source
+ * applies to each source component when calc_phase is true -- on GPU `device`,
+ * without allocating any device memory.  It is meant for callers that cannot
+ * allocate: a process whose device memory is already committed to a memory
+ * pool or to resident solves, or a thread preparing sources while solves run
+ * on other streams (the cudaFree behind FDTD_add_source's temporary buffer
+ * waits for all work on the device).  Convert the six components with it, then
+ * register them with FDTD_add_source(..., calc_phase = false).
+ *   stream: a cudaStream_t of `device`, or NULL for the calling thread's
+ *           default stream; the call returns after that stream has finished.
+ *   msg:    optional buffer (msglen bytes) for an error message.
+ * n above FDTD_NOALLOC_MAX_VALUES fails with FDTD_ERR_ARG.  Every GPU that
+ * loads this library holds the 8 MiB array until the process exits.  The first
+ * call on a device looks up the array's address there (set-up); make it before
+ * any stream capture.  All calls on a device share the array, so calls that
+ * overlap in time (from several host threads) race and must be serialised. */
+int FDTD_amp_phase_noalloc(int device, void *stream, fdtd_complex128 *a, long long n, char *msg,
+                           int msglen);
+
 #ifdef __cplusplus
 }
 #endif
