@@ -723,7 +723,7 @@ int FDTD_set_precision(FDTDHandle* h, int bits) {
 }
 
 int FDTD_set_kernel(FDTDHandle* h, int which) {
-    if (which < 0 || which > 5) return h->fail(FDTD_ERR_ARG, "kernel must be in 0..5");
+    if (which < 0 || which > 7) return h->fail(FDTD_ERR_ARG, "kernel must be in 0..7");
     h->kernel = which;
     return FDTD_OK;
 }
@@ -992,11 +992,20 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     bool small_index = (long long)h->Nz * h->Ny * ((h->Nx + 31) / 32 * 32) < (1LL << 31) &&
                        (long long)h->Nz * h->Ny * (h->w[0] + h->w[1]) < (1LL << 31);
     // kernel ids: 0 auto, 1 scalar H/E pair, 2 fused CTA tiles (plain loads),
-    // 3 fused CTA tiles (TMA), 4 fused warp tiles, 5 vector H/E pair
+    // 3 fused CTA tiles (TMA), 4 fused warp tiles, 5 vector H/E pair,
+    // 6 16-byte-vector H/E pair over flattened rows, 7 streaming H/E pair
+    // (row tiles through a bulk-copy ring)
     int kid = h->kernel == 0 ? 5 : h->kernel;
     if (periodic || !small_index) kid = 1;
     if (kid == 3 && encode_fn() == nullptr) kid = 5;
+    if (kid == 6) {
+        int nv;
+        unsigned mg;
+        if (!fdtdb::v16_magic(h->Nx, h->Ny, sizeof(T) == 4 ? 4 : 2, &nv, &mg)) kid = 5;
+    }
     bool vec = kid == 5;
+    bool v16 = kid == 6;
+    bool strm = kid == 7;
     bool warp = kid == 4;
     bool tma = kid == 3;
     bool fused = kid == 2 || kid == 3 || kid == 4;
@@ -1062,6 +1071,12 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     if (tma) wz = zchunk;
     fdtdb::GridView<T> g0 = make_view<T>(h, r, 0);
     fdtdb::GridView<T> g1 = fused ? make_view<T>(h, r, 1) : g0;
+    fdtdb::StreamPlan splan;
+    if (strm && fdtdb::stream_plan<T>(g0, h->zchunk, &splan) != cudaSuccess) {
+        cudaGetLastError();
+        strm = false;
+        vec = true;
+    }
     T* f0[6];
     T* f1[6];
     for (int c = 0; c < 6; c++) {
@@ -1088,6 +1103,11 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
                 bool odd = n & 1;
                 fdtdb::launch_step_fused<T>(odd ? g1 : g0, odd ? g0 : g1, odd ? f1 : f0,
                                             odd ? f0 : f1, src, sb, (int)q, h->stream);
+            } else if (strm) {
+                CK(fdtdb::launch_step_stream<T>(g0, f0, src, sb, (int)q, splan, dptr<int>(r.err),
+                                                h->stream));
+            } else if (v16) {
+                CK(fdtdb::launch_step_v16<T>(g0, f0, src, sb, (int)q, h->stream));
             } else if (vec) {
                 CK(fdtdb::launch_step_vec<T>(g0, f0, src, sb, (int)q, h->stream));
             } else {
@@ -1185,7 +1205,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     res->device_ms = ms_steps;
     res->total_ms = ms_total;
     res->launches = launches;
-    res->zchunk = (warp || tma) ? wz : 0;
+    res->zchunk = (warp || tma) ? wz : (strm ? splan.R : 0);
     res->status = FDTD_OK;
     if (!fixed && not_converged()) {
         bool bad = std::isnan(Ach) || std::isinf(Ach) || std::isnan(Pch) || std::isinf(Pch);

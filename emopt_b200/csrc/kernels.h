@@ -18,6 +18,37 @@ template <typename T>
 cudaError_t launch_step_vec(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
                             const long long* step_base, int off, cudaStream_t st);
 
+// H and E half-steps with one 16-byte vector (4 floats / 2 doubles) of x cells
+// per thread over flattened (row, vector) pairs (vec4_kernels.cu).  Requires
+// non-periodic boundaries; returns cudaErrorInvalidValue when the row split
+// of the flattened index cannot be done exactly for this grid (v16_magic).
+template <typename T>
+cudaError_t launch_step_v16(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
+                            const long long* step_base, int off, cudaStream_t st);
+bool v16_magic(int Nx, int Ny, int V, int* nvec, unsigned* magic);
+
+// Streaming H/E pair (stream_kernels.cu): persistent CTAs, row tiles fetched
+// by bulk async copies into a shared-memory ring.  stream_plan fixes the tile
+// rows (rows_hint > 0 caps them), the ring depth and the launch shape for a
+// grid on the current device (once per solve); launch_step_stream runs one
+// time step.  Requires non-periodic boundaries.
+struct StreamPlan {
+    int R, S;              // rows per tile, ring stages
+    int nty, ntiles;       // tiles per plane, tiles in total
+    int nvr;               // 16-byte vectors per row covering Nx
+    unsigned magic;        // q / nvr == umulhi(q, magic) for every q of a tile
+    int stage_bytes, smem, threads, grid;
+    int slot[16];          // byte offset of each array in a stage (this kernel)
+    int hslot[16], eslot[16];
+    int hbox[4], ebox[4];  // planes [0,1) x rows [2,3) reached by M / J sources
+};
+template <typename T>
+cudaError_t stream_plan(const GridView<T>& g, int rows_hint, StreamPlan* plan);
+template <typename T>
+cudaError_t launch_step_stream(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
+                               const long long* step_base, int off, const StreamPlan& plan,
+                               int* err, cudaStream_t st);
+
 // One fused time step reading set A (ga's CPML state, fields fa) and writing
 // set B (gb's CPML state, fields fb).  Requires non-periodic boundaries.
 template <typename T>

@@ -8,10 +8,19 @@
 // boundary comes from the adjacent lane with a warp shuffle; only the last
 // lane of a warp (first lane for the E update) loads it separately.  Each
 // thread issues all of its loads before any dependent instruction, and the
-// source test is made once per block before any per-cell work.  Requires
-// non-periodic boundaries (the solver uses k_update_H / k_update_E otherwise).
+// source test is made once per block before any per-cell work.  Blocks are
+// single warps (one row each): a finished warp frees its slot at once, which
+// keeps more loads in flight than 8-warp blocks whose slot waits for the
+// slowest warp (124 us against 137 us per step on the 321 x 161 x 101 MMI
+// block in fp32).  Requires non-periodic boundaries (the solver uses
+// k_update_H / k_update_E otherwise).
 #include "cell.cuh"
 #include "kernels.h"
+
+// Rows of a plane per block (blockDim.y, one warp per row).
+#ifndef VEC_BLOCK_ROWS
+#define VEC_BLOCK_ROWS 1
+#endif
 
 namespace fdtdb {
 
@@ -69,7 +78,7 @@ __device__ __forceinline__ bool sources_touch(const SourceList<T>& src, int comp
 
 }  // namespace
 
-// One thread: cells k0 .. k0+V-1 of row j, plane i.  blockDim = (32, 8):
+// One thread: cells k0 .. k0+V-1 of row j, plane i.  blockDim = (32, VEC_BLOCK_ROWS):
 // x over vectors of a row, y over rows; grid.z over planes.
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_H_vec(GridView<T> g, Fields<T> f, SourceList<T> src,
@@ -77,7 +86,7 @@ __global__ void __launch_bounds__(256) k_update_H_vec(GridView<T> g, Fields<T> f
     constexpr int V = V16<T>::N;
     constexpr unsigned FULL = 0xffffffffu;
     const int m = blockIdx.x * 32 + threadIdx.x;
-    const int j = blockIdx.y * 8 + threadIdx.y;
+    const int j = blockIdx.y * VEC_BLOCK_ROWS + threadIdx.y;
     const int i = blockIdx.z;
     const int k0 = m * V;
     const int lane = threadIdx.x;
@@ -126,7 +135,7 @@ __global__ void __launch_bounds__(256) k_update_H_vec(GridView<T> g, Fields<T> f
     T mx[V], my[V], mz[V];
     const bool mu_arr = g.bHarr[0] != nullptr;
     if (mu_arr && act) { vload<T>(mx, g.bHarr[0] + p); vload<T>(my, g.bHarr[1] + p); vload<T>(mz, g.bHarr[2] + p); }
-    const bool srcb = src.n && sources_touch<T>(src, 3, i, blockIdx.y * 8, blockIdx.y * 8 + 8,
+    const bool srcb = src.n && sources_touch<T>(src, 3, i, blockIdx.y * VEC_BLOCK_ROWS, (blockIdx.y + 1) * VEC_BLOCK_ROWS,
                                                 blockIdx.x * 32 * V, (blockIdx.x + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_base + off];
@@ -204,7 +213,7 @@ __global__ void __launch_bounds__(256) k_update_E_vec(GridView<T> g, Fields<T> f
     constexpr int V = V16<T>::N;
     constexpr unsigned FULL = 0xffffffffu;
     const int m = blockIdx.x * 32 + threadIdx.x;
-    const int j = blockIdx.y * 8 + threadIdx.y;
+    const int j = blockIdx.y * VEC_BLOCK_ROWS + threadIdx.y;
     const int i = blockIdx.z;
     const int k0 = m * V;
     const int lane = threadIdx.x;
@@ -251,7 +260,7 @@ __global__ void __launch_bounds__(256) k_update_E_vec(GridView<T> g, Fields<T> f
             px2[e] = ld(PX.psi[2] + s); px3[e] = ld(PX.psi[3] + s);
         }
     }
-    const bool srcb = src.n && sources_touch<T>(src, 0, i, blockIdx.y * 8, blockIdx.y * 8 + 8,
+    const bool srcb = src.n && sources_touch<T>(src, 0, i, blockIdx.y * VEC_BLOCK_ROWS, (blockIdx.y + 1) * VEC_BLOCK_ROWS,
                                                 blockIdx.x * 32 * V, (blockIdx.x + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_base + off];
@@ -342,8 +351,8 @@ cudaError_t launch_step_vec(const GridView<T>& g, T* const* fields, const Source
     Fields<T> f;
     for (int c = 0; c < 6; c++) f.c[c] = fields[c];
     const int nvec = (g.Nx + V - 1) / V;
-    dim3 block(32, 8);
-    dim3 grid((nvec + 31) / 32, (g.Ny + 7) / 8, g.Nz);
+    dim3 block(32, VEC_BLOCK_ROWS);
+    dim3 grid((nvec + 31) / 32, (g.Ny + VEC_BLOCK_ROWS - 1) / VEC_BLOCK_ROWS, g.Nz);
     k_update_H_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
     k_update_E_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
     return cudaGetLastError();

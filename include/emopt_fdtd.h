@@ -111,8 +111,10 @@ int FDTD_last_error(FDTDHandle *h, char *buf, int buflen);
  * device).  Must precede the first call that touches the device. */
 int FDTD_set_device(FDTDHandle *h, int device);
 
-/* Planes per CTA of the fused time-step kernels (0 = chosen from the
- * occupancy, the default).  A tuning knob; results do not depend on it. */
+/* Planes per CTA of the fused time-step kernels, or the largest number of
+ * rows per tile of the streaming kernel (0 = chosen from the occupancy or
+ * the shared memory, the default).  A tuning knob; results do not depend on
+ * it. */
 int FDTD_set_zchunk(FDTDHandle *h, int planes);
 
 /* Storage/arithmetic precision of FDTD_solve_cw: 64 (default, the reference's
@@ -123,8 +125,11 @@ int FDTD_set_precision(FDTDHandle *h, int bits);
 /* Time-stepping kernel of FDTD_solve_cw: 0 = automatic (default), 1 = H and
  * E kernels with one cell per thread, 2 = fused CTA-tile kernel with plain
  * loads, 3 = fused CTA-tile kernel with TMA-staged planes, 4 = fused kernel on
- * warp-independent register tiles, 5 = H and E kernels with one 16-byte
- * vector of x cells per thread.  Periodic boundaries always use 1. */
+ * warp-independent register tiles, 5 = H and E kernels with one 2-element
+ * vector of x cells per thread, 6 = H and E kernels with one 16-byte vector
+ * per thread over flattened rows, 7 = persistent H and E kernels streaming
+ * row tiles through a shared-memory ring filled by bulk async copies.
+ * Periodic boundaries always use 1. */
 int FDTD_set_kernel(FDTDHandle *h, int which);
 
 typedef struct {
@@ -147,7 +152,7 @@ typedef struct {
     double device_ms;          /* device time of all time steps (CUDA events) */
     double total_ms;           /* device time of the whole call incl. transfers */
     long long launches;        /* kernels this call launched */
-    int zchunk;                /* planes per CTA used by the fused kernel (0: not fused) */
+    int zchunk;                /* planes per CTA of a fused kernel, rows per tile of the streaming kernel (else 0) */
     int status;                /* FDTD_OK, FDTD_NMAX or FDTD_NONFINITE */
 } FDTDSolveResult;
 

@@ -86,5 +86,5 @@ def test_argument_errors_are_reported():
     h = ct.libFDTD.FDTD_new()
     assert ct.libFDTD.FDTD_set_precision(h, 16) == ct.FDTD_ERR_ARG
     assert "precision" in ct.last_error(h)[1]
-    assert ct.libFDTD.FDTD_set_kernel(h, 7) == ct.FDTD_ERR_ARG
+    assert ct.libFDTD.FDTD_set_kernel(h, 8) == ct.FDTD_ERR_ARG
     ct.libFDTD.FDTD_delete(h)

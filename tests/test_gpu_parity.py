@@ -115,7 +115,7 @@ def test_abi_per_call_field_arrays_match_oracle_each_step():
 
 
 # ------------------------------------------------ device-resident solve
-@pytest.mark.parametrize("kernel", ["vector", "scalar", "fused_plain", "fused_tma", "fused_warp"])
+@pytest.mark.parametrize("kernel", ["stream", "vector16", "vector", "scalar", "fused_plain", "fused_tma", "fused_warp"])
 @pytest.mark.parametrize("name", list(BOX_KW))
 def test_solve_cw_fp64_matches_golden(name, kernel):
     g = golden(f"box_{name}.npz")
@@ -125,7 +125,7 @@ def test_solve_cw_fp64_matches_golden(name, kernel):
     assert rel_l2(F, g["fields"]) < 1e-11
 
 
-@pytest.mark.parametrize("kernel", ["vector", "scalar", "fused_plain", "fused_tma", "fused_warp"])
+@pytest.mark.parametrize("kernel", ["stream", "vector16", "vector", "scalar", "fused_plain", "fused_tma", "fused_warp"])
 def test_solve_cw_fp64_converging_step_count(kernel):
     """Run to rtol = 1e-6: the step count is bit-for-bit the reference's."""
     g = golden("box_converge.npz")
@@ -159,7 +159,7 @@ def test_solve_cw_waveguide_full_field_vs_oracle():
     p = P.waveguide()
     ref = np.stack(oracle_for(p, oracle_lib()).run_fixed_slabs(p.fixed_steps,
                                                                min(32, os.cpu_count() or 1))["fields"])
-    for kern in ("vector", "scalar", "fused_plain", "fused_tma", "fused_warp"):
+    for kern in ("stream", "vector16", "vector", "scalar", "fused_plain", "fused_tma", "fused_warp"):
         F64, _, _ = solve_gpu(p, "fp64", kern)
         assert rel_l2(F64, ref) < 1e-9, kern
     F32, _, _ = solve_gpu(p, "fp32", "auto")
@@ -168,7 +168,7 @@ def test_solve_cw_waveguide_full_field_vs_oracle():
     assert err32 < 1e-4
 
 
-@pytest.mark.parametrize("kernel", ["vector", "scalar", "fused_tma", "fused_warp"])
+@pytest.mark.parametrize("kernel", ["stream", "vector16", "vector", "scalar", "fused_tma", "fused_warp"])
 def test_fp32_box_error(kernel):
     g = golden("box_converge.npz")
     p = P.random_box(seed=11, shape=(10, 12, 15), fixed_steps=None, rtol=1e-6)
