@@ -437,7 +437,7 @@ static int legacy_upload_source_arrays(FDTDHandle* h, std::vector<fdtdb::LegacyS
         for (int c = 0; c < 6; c++) {
             DevBuf& b = h->lsrc[6 * s + c];
             CK(b.ensure(sizeof(c128) * (n > 0 ? n : 1)));
-            if (n > 0) CK(cudaMemcpyAsync(b.p, hs.comp[c], sizeof(c128) * n, cudaMemcpyHostToDevice, h->stream));
+            if (n > 0) CK(cudaMemcpyAsync(b.p, hs.comp[c], sizeof(c128) * n, cudaMemcpyDefault, h->stream));
             ls.comp[c] = dptr<c128>(b);
         }
         ls.i0 = hs.i0; ls.j0 = hs.j0; ls.k0 = hs.k0; ls.I = hs.I; ls.J = hs.J; ls.K = hs.K;
@@ -472,7 +472,7 @@ static int legacy_view(FDTDHandle* h, fdtdb::LegacyView& v) {
                 size_t n = h->tab[a][q].size();
                 CK(h->ltab[a][q].ensure(sizeof(double) * (n ? n : 1)));
                 if (n) CK(cudaMemcpyAsync(h->ltab[a][q].p, h->tab[a][q].data(), sizeof(double) * n,
-                                          cudaMemcpyHostToDevice, h->stream));
+                                          cudaMemcpyDefault, h->stream));
             }
         CK(cudaStreamSynchronize(h->stream));
         h->ltab_dirty = false;
@@ -496,17 +496,17 @@ static int legacy_in(FDTDHandle* h, bool need_eps, bool need_mu) {
         if (!h->hE[c] || !h->hH[c]) return h->fail(FDTD_ERR_ARG, "field arrays are not set");
         CK(h->lE[c].ensure(sizeof(double) * np));
         CK(h->lH[c].ensure(sizeof(double) * np));
-        CK(cudaMemcpyAsync(h->lE[c].p, h->hE[c], sizeof(double) * np, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaMemcpyAsync(h->lH[c].p, h->hH[c], sizeof(double) * np, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->lE[c].p, h->hE[c], sizeof(double) * np, cudaMemcpyDefault, h->stream));
+        CK(cudaMemcpyAsync(h->lH[c].p, h->hH[c], sizeof(double) * np, cudaMemcpyDefault, h->stream));
         if (need_eps) {
             if (!h->heps[c]) return h->fail(FDTD_ERR_ARG, "material arrays are not set");
             CK(h->leps[c].ensure(sizeof(c128) * n));
-            CK(cudaMemcpyAsync(h->leps[c].p, h->heps[c], sizeof(c128) * n, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(h->leps[c].p, h->heps[c], sizeof(c128) * n, cudaMemcpyDefault, h->stream));
         }
         if (need_mu) {
             if (!h->hmu[c]) return h->fail(FDTD_ERR_ARG, "material arrays are not set");
             CK(h->lmu[c].ensure(sizeof(c128) * n));
-            CK(cudaMemcpyAsync(h->lmu[c].p, h->hmu[c], sizeof(c128) * n, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(h->lmu[c].p, h->hmu[c], sizeof(c128) * n, cudaMemcpyDefault, h->stream));
         }
     }
     return FDTD_OK;
@@ -515,8 +515,8 @@ static int legacy_in(FDTDHandle* h, bool need_eps, bool need_mu) {
 static int legacy_out(FDTDHandle* h) {
     long long np = h->npad();
     for (int c = 0; c < 3; c++) {
-        CK(cudaMemcpyAsync(h->hE[c], h->lE[c].p, sizeof(double) * np, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(h->hH[c], h->lH[c].p, sizeof(double) * np, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(h->hE[c], h->lE[c].p, sizeof(double) * np, cudaMemcpyDefault, h->stream));
+        CK(cudaMemcpyAsync(h->hH[c], h->lH[c].p, sizeof(double) * np, cudaMemcpyDefault, h->stream));
     }
     return h->sync_check("legacy half step");
 }
@@ -545,7 +545,7 @@ static int legacy_snap_in(FDTDHandle* h, c128* const* host, DevBuf* dev, c128** 
     for (int c = 0; c < 6; c++) {
         if (!host[c]) return h->fail(FDTD_ERR_ARG, "t0/t1 arrays are not set");
         CK(dev[c].ensure(sizeof(c128) * n));
-        CK(cudaMemcpyAsync(dev[c].p, host[c], sizeof(c128) * n, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(dev[c].p, host[c], sizeof(c128) * n, cudaMemcpyDefault, h->stream));
         out[c] = dptr<c128>(dev[c]);
     }
     return FDTD_OK;
@@ -554,7 +554,7 @@ static int legacy_snap_in(FDTDHandle* h, c128* const* host, DevBuf* dev, c128** 
 static int legacy_snap_out(FDTDHandle* h, c128* const* host, DevBuf* dev) {
     long long n = h->ncells();
     for (int c = 0; c < 6; c++)
-        CK(cudaMemcpyAsync(host[c], dev[c].p, sizeof(c128) * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(host[c], dev[c].p, sizeof(c128) * n, cudaMemcpyDefault, h->stream));
     return h->sync_check("snapshot");
 }
 
@@ -622,10 +622,10 @@ void FDTD_add_source(FDTDHandle* h, fdtd_complex128* Jx, fdtd_complex128* Jy, fd
     DevBuf tmp;
     cudaError_t e = tmp.ensure(sizeof(c128) * n);
     for (int c = 0; c < 6 && e == cudaSuccess; c++) {
-        e = cudaMemcpyAsync(tmp.p, s.comp[c], sizeof(c128) * n, cudaMemcpyHostToDevice, h->stream);
+        e = cudaMemcpyAsync(tmp.p, s.comp[c], sizeof(c128) * n, cudaMemcpyDefault, h->stream);
         if (e != cudaSuccess) break;
         fdtdb::launch_amp_phase(dptr<c128>(tmp), n, h->stream);
-        e = cudaMemcpyAsync(s.comp[c], tmp.p, sizeof(c128) * n, cudaMemcpyDeviceToHost, h->stream);
+        e = cudaMemcpyAsync(s.comp[c], tmp.p, sizeof(c128) * n, cudaMemcpyDefault, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     }
     if (e == cudaSuccess) e = cudaGetLastError();
@@ -828,7 +828,7 @@ int prepare_materials(FDTDHandle* h, Resident<T>& r) {
         if (!h->heps[c] || !h->hmu[c]) return h->fail(FDTD_ERR_ARG, "material arrays are not set");
         // pitched arrays: zero the row padding once so that every element is defined
         CK(cudaMemsetAsync(r.bE[c].p, 0, sizeof(T) * cells, h->stream));
-        CK(cudaMemcpyAsync(r.stage.p, h->heps[c], sizeof(c128) * n, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(r.stage.p, h->heps[c], sizeof(c128) * n, cudaMemcpyDefault, h->stream));
         T* a_out = nullptr;
         if (h->lossy) {
             CK(r.aE[c].ensure(sizeof(T) * cells));
@@ -838,14 +838,14 @@ int prepare_materials(FDTDHandle* h, Resident<T>& r) {
         fdtdb::launch_material_coeffs<T>(dptr<c128>(r.stage), nullptr, h->Nx, h->Ny, h->Nz, r.px,
                                          h->dt, h->lossy, dptr<T>(r.bE[c]), a_out, nullptr, h->stream);
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(r.stage.p, h->hmu[c], sizeof(c128) * n, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(r.stage.p, h->hmu[c], sizeof(c128) * n, cudaMemcpyDefault, h->stream));
         int one = 1;
-        CK(cudaMemcpyAsync(r.flag.p, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(r.flag.p, &one, sizeof(int), cudaMemcpyDefault, h->stream));
         fdtdb::launch_uniform_check(dptr<c128>(r.stage), n, dptr<int>(r.flag), h->stream);
         int uniform = 0;
         c128 first;
-        CK(cudaMemcpyAsync(&uniform, r.flag.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(&first, r.stage.p, sizeof(c128), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(&uniform, r.flag.p, sizeof(int), cudaMemcpyDefault, h->stream));
+        CK(cudaMemcpyAsync(&first, r.stage.p, sizeof(c128), cudaMemcpyDefault, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         r.mu_uniform[c] = uniform != 0;
         r.mu_value[c] = first.real;
@@ -875,7 +875,7 @@ int prepare_materials(FDTDHandle* h, Resident<T>& r) {
         for (int q = 0; q < 6; q++) {
             CK(r.tab[a][q].ensure(sizeof(T) * t[q].size()));
             CK(cudaMemcpyAsync(r.tab[a][q].p, t[q].data(), sizeof(T) * t[q].size(),
-                               cudaMemcpyHostToDevice, h->stream));
+                               cudaMemcpyDefault, h->stream));
         }
         CK(cudaStreamSynchronize(h->stream));
     }
@@ -912,7 +912,7 @@ int prepare_sources(FDTDHandle* h, Resident<T>& r, fdtdb::SourceList<T>& list) {
             DevBuf& co = r.src_coef[6 * s + c];
             CK(ap.ensure(sizeof(c128) * n));
             CK(co.ensure(sizeof(T) * 2 * n));
-            CK(cudaMemcpyAsync(ap.p, hs.comp[c], sizeof(c128) * n, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(ap.p, hs.comp[c], sizeof(c128) * n, cudaMemcpyDefault, h->stream));
             const T* coef_arr;
             double coef_s = 0;
             if (c < 3) {
@@ -1056,7 +1056,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     CK(cudaMemsetAsync(r.pout.p, 0, sizeof(double) * 4, h->stream));
     std::vector<long long> map((size_t)nc, -1);
     for (int q = 0; q < nconv; q++) map[q] = probe_offset(h, r.px, o->conv_pts[q]);
-    CK(cudaMemcpyAsync(r.pmap.p, map.data(), sizeof(long long) * nc, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(r.pmap.p, map.data(), sizeof(long long) * nc, cudaMemcpyDefault, h->stream));
     CK(cudaStreamSynchronize(h->stream));   // map is a stack vector
     fdtdb::ProbeDev pd;
     pd.win = dptr<double>(r.pwin); pd.A = dptr<double>(r.pA);
@@ -1143,14 +1143,14 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
         n += Tn;
         nprobes++;
         if (!fixed) {
-            CK(cudaMemcpyAsync(h->pinned, r.pout.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(h->pinned, r.pout.p, sizeof(double) * 2, cudaMemcpyDefault, h->stream));
             CK(cudaStreamSynchronize(h->stream));
             Ach = h->pinned[0];
             Pch = h->pinned[1];
         }
     }
     if (fixed) {
-        CK(cudaMemcpyAsync(h->pinned, r.pout.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(h->pinned, r.pout.p, sizeof(double) * 2, cudaMemcpyDefault, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         Ach = h->pinned[0];
         Pch = h->pinned[1];
@@ -1178,20 +1178,20 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
                                     dptr<c128>(r.stage), h->stream);
         launches++;
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(h->ht0[c], r.stage.p, sizeof(c128) * ncell, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(h->ht0[c], r.stage.p, sizeof(c128) * ncell, cudaMemcpyDefault, h->stream));
     }
     if (o->copy_t1) {
         for (int c = 0; c < 6; c++) {
             if (!h->ht1[c]) return h->fail(FDTD_ERR_ARG, "t1 arrays are not set");
-            CK(cudaMemcpyAsync(r.stage.p, h->ht1[c], sizeof(c128) * ncell, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(r.stage.p, h->ht1[c], sizeof(c128) * ncell, cudaMemcpyDefault, h->stream));
             fdtdb::launch_snapshot_real<T>(dptr<T>(r.snap[1][c]), h->Nx, h->Ny, h->Nz, r.px,
                                            dptr<c128>(r.stage), h->stream);
-            CK(cudaMemcpyAsync(h->ht1[c], r.stage.p, sizeof(c128) * ncell, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(h->ht1[c], r.stage.p, sizeof(c128) * ncell, cudaMemcpyDefault, h->stream));
         }
     }
     CK(cudaEventRecord(h->ev[3], h->stream));
     int kerr = 0;
-    CK(cudaMemcpyAsync(&kerr, r.err.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&kerr, r.err.p, sizeof(int), cudaMemcpyDefault, h->stream));
     if ((rc = h->sync_check("FDTD_solve_cw")) != FDTD_OK) return rc;
     if (kerr) return h->fail(FDTD_ERR_CUDA, "a bounded wait in the step kernel gave up (code %d)", kerr);
     float ms_steps = 0, ms_total = 0;

@@ -143,10 +143,13 @@ libFDTD.FDTD_amp_phase_noalloc.argtypes = [c_int, c_void_p,
                                            c_longlong, c_char_p, c_int]
 libFDTD.FDTD_amp_phase_noalloc.restype = c_int
 NOALLOC_MAX_VALUES = 524288
+libFDTD.FDTD_grad_eps.argtypes = [c_int, c_void_p, POINTER(c_void_p), POINTER(c_void_p), c_int,
+                                  c_int, c_int, POINTER(c_int), c_int, c_void_p, c_char_p, c_int]
+libFDTD.FDTD_grad_eps.restype = c_int
 
 ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_zchunk",
                  "FDTD_set_precision", "FDTD_set_kernel", "FDTD_solve_cw",
-                 "FDTD_amp_phase_noalloc")
+                 "FDTD_amp_phase_noalloc", "FDTD_grad_eps")
 
 
 class FDTDError(RuntimeError):

@@ -164,6 +164,53 @@ def mmi_block(seed: int = 0, nd=(120, 80), rtol: float = 1e-6,
     return p
 
 
+def mmi_gradient(seed: int = 1, nd=(80, 80), d: float = 0.025, w_pml: int = 20,
+                 rtol: float = 1e-6, fixed_steps: int | None = None) -> Problem:
+    """Differentiation workload: the MMI block with a seeded uniform[0,1]
+    design density on an ``nd`` grid (blur sigma = 2 cells, tanh projection
+    beta = 8, eta = 0.5), the Jy Gaussian sheet in the lower input guide and a
+    mode-match figure of merit on the output plane x = 7.0 um against a fixed
+    Gaussian (w0 = 0.35 um) centred on the upper output guide: Ey = G,
+    Hz = n_clad G with n_clad = sqrt(2.085) (not power-normalised).
+
+    Extra attributes: ``design_params`` (the density), ``design_rect`` (um),
+    ``design_layer`` (zc, half height), ``fom_plane`` (indices k, j1, j2, i1,
+    i2 of the x-normal plane, the part outside the CPML) and ``fom_mode``
+    (dict of mode fields on it).
+    The default is the full 321 x 161 x 101 grid; ``d = 0.05, w_pml = 10``
+    gives a 161 x 81 x 51 version of the same geometry for tests."""
+    X, Y, Z = 8.0, 4.0, 2.5
+    p = Problem(f"mmi_grad_d{d}", X, Y, Z, d, d, d, 1.55, w_pml=(w_pml,) * 6, rtol=rtol,
+                fixed_steps=fixed_steps)
+    shape = p.shape
+    Nz, Ny, Nx = shape
+    rng = np.random.default_rng(seed)
+    p.design_params = rng.uniform(0.0, 1.0, nd)
+    rho = projected_density(p.design_params)
+    p.mats = sample_yee(mmi_geometry(rho, shape, d), shape, d, d, d)
+    xc, yc, zc = (Nx - 1) * d / 2, (Ny - 1) * d / 2, (Nz - 1) * d / 2
+    p.sources = [gaussian_sheet(shape, int(round(1.0 / d)), d, d, yc - 0.5, zc, 0.35)]
+    p.design_rect = (xc - 1.5, xc + 1.5, yc - 1.0, yc + 1.0)
+    p.design_layer = (zc, 0.11)
+    p.design_nd = tuple(nd)
+    k = int(round(7.0 / d))
+    p.fom_plane = (k, w_pml, Ny - w_pml, w_pml, Nz - w_pml)   # outside the CPML
+    z = np.arange(w_pml, Nz - w_pml) * d
+    y = np.arange(w_pml, Ny - w_pml) * d
+    Zg, Yg = np.meshgrid(z, y, indexing="ij")
+    G = np.exp(-((Yg - (yc + 0.5)) ** 2 + (Zg - zc) ** 2) / 0.35 ** 2).astype(np.complex128)
+    p.fom_mode = {"Ey": G[:, :, None], "Hz": np.sqrt(EPS_SIO2) * G[:, :, None]}
+    return p
+
+
+def design_eps(p: Problem, params: np.ndarray):
+    """The three eps arrays of :func:`mmi_gradient`'s geometry for a design density."""
+    Nz, Ny, Nx = p.shape
+    mats = sample_yee(mmi_geometry(projected_density(params), p.shape, p.dx), p.shape,
+                      p.dx, p.dy, p.dz)
+    return mats[:3]
+
+
 def random_box(seed: int, shape=(9, 11, 14), d=0.04, w_pml=(3, 4, 3, 2, 3, 4), bc="000",
                complex_eps=False, fixed_steps: int | None = 120, mu_random=False,
                n_sources=1, rtol=1e-6) -> Problem:

@@ -156,12 +156,39 @@ typedef struct {
     int status;                /* FDTD_OK, FDTD_NMAX or FDTD_NONFINITE */
 } FDTDSolveResult;
 
-/* Device-resident CW solve: equivalent to FDTD_reset_pml, zeroing the fields
+/* Caller arrays (fields, materials, t0/t1 arrays, sources) may live in host
+ * memory or in device memory of the handle's device: every copy between them
+ * and the library's device buffers lets the CUDA runtime infer the direction.
+ *
+ * Device-resident CW solve: equivalent to FDTD_reset_pml, zeroing the fields
  * and the loop of emopt/fdtd.py:1016-1194 (probe window, norm test, capture of
  * t0 and t1 Tn steps apart, 3-sample extraction), run on the GPU.  Reads the
  * material arrays and the sources registered with FDTD_add_source; writes the
  * complex steady-state fields into the t0 arrays.  Returns a status. */
 int FDTD_solve_cw(FDTDHandle *h, const FDTDSolveOptions *opt, FDTDSolveResult *res);
+
+/* Permittivity factor of the adjoint gradient, fused over a design box.  No
+ * counterpart in the reference as one call: it evaluates, per cell and E
+ * component c, g_c = -2 Re(1j * adj_c * fwd_c) = 2 Im(adj_c * fwd_c), the
+ * derivative of the objective per unit real change of eps_c in the adjoint
+ * product of emopt/fdtd.py:1694-1717 (gradient -2 Re(y^T dA x),
+ * emopt/adjoint_method.py:505-544).
+ *   fwd, adj: three pointers each (Ex, Ey, Ez) to complex128 [Nz][Ny][Nx]
+ *             arrays in device memory of `device`, e.g. t0 arrays that
+ *             FDTD_solve_cw wrote;
+ *   box:      10 ints: k0, k1, j0, j1 (x and y ranges, half open) and the z
+ *             range [i0_c, i1_c) of each component c = 0, 1, 2;
+ *   planar:   1: out[c][j-j0][k-k0] = sum over i in [i0_c, i1_c) of g_c
+ *             (Kahan-compensated float64); 0: out[c][i-imin][j-j0][k-k0] with
+ *             imin / imax the smallest / largest z bound, zero outside a
+ *             component's range;
+ *   out:      float64 device memory of `device`;
+ *   stream:   a cudaStream_t of `device` or NULL (the calling thread's default
+ *             stream); the call returns after the kernel has finished.
+ * Returns FDTD_OK, FDTD_ERR_ARG or FDTD_ERR_CUDA, with a message in msg. */
+int FDTD_grad_eps(int device, void *stream, const fdtd_complex128 *const *fwd,
+                  const fdtd_complex128 *const *adj, int Nx, int Ny, int Nz, const int *box,
+                  int planar, double *out, char *msg, int msglen);
 
 /* Largest n accepted by FDTD_amp_phase_noalloc: 524288 complex128 values, the
  * 8 MiB device array it stages through. */
