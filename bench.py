@@ -49,8 +49,13 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--kernel", default="auto", choices=["auto", "scalar", "fused_plain", "fused_tma", "fused_warp", "vector"])
-    ap.add_argument("--workload", default="mmi", choices=["mmi", "waveguide"])
+    ap.add_argument("--kernel", default="auto",
+                    choices=["auto", "scalar", "fused_plain", "fused_tma", "fused_warp", "vector",
+                             "vector16", "stream"])
+    ap.add_argument("--workload", default="mmi", choices=["mmi", "waveguide", "serving", "grad"])
+    ap.add_argument("--requests", type=int, default=512, help="serving: requests in the stream")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: mean arrivals per second")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the fp64 comparison solve")
     return ap.parse_args()
@@ -337,10 +342,103 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_serving(args):
+    """Serving form: a Poisson stream of CW solves of mixed grids and
+    wavelengths through the continuous-batching engine (FDTD_serve_*)."""
+    world, rank, local = dist_setup(args.gpus)
+    from emopt_b200 import serving as S
+    specs = S.poisson_stream(args.requests, args.rate, seed=3 + rank)
+    # warm-up: two small requests through a throw-away engine (graph, kernels, allocator)
+    warm = S.ServeEngine(local, 8e9, 8, 32)
+    S.run_stream(S.poisson_stream(2, 1e9, seed=99, shape=(40, 40, 48), w_pml=8), warm, realtime=False)
+    warm.close()
+    eng = S.ServeEngine(local, args.budget_gb * 1e9, 128, 32)
+    barrier(world)
+    with ClockSampler(local) as clk:
+        out = S.run_stream(specs, eng, realtime=True)
+    barrier(world)
+    eng.close()
+    (makespan,) = barrier_max([out["makespan"]], world)
+    (cu,) = barrier_sum([out["cell_updates"]], world)
+    value = cu / makespan / 1e9
+    steps = [r["steps"] for r in out["results"].values()]
+    result = {
+        "metric": "serving: aggregate Gcell-updates/s with p50/p99 latency (CW-FDTD requests, "
+                  "Poisson arrivals, mixed grids 64^3..384x256x128, fp32, rtol=1e-6)",
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": len(steps), "warmup": 2,
+        "ms_per_step": 1e3 * makespan / max(len(steps), 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving_stream", "requests": args.requests, "rate_per_s": args.rate,
+                   "budget_gb": args.budget_gb, "steps_per_replay": 32, "seed": 3,
+                   "parallelism": f"replicas{world}"},
+        "latency_s": {"p50": out["p50"], "p99": out["p99"], "max": float(out["latency"].max()),
+                      "mean": float(out["latency"].mean())},
+        "makespan_s": makespan,
+        "time_steps": {"total": int(sum(steps)), "median": float(np.median(steps)),
+                       "max": int(max(steps))},
+        "nmax_hits": int(sum(1 for r in out["results"].values() if r["status"] != 0)),
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_grad(args):
+    """Differentiation form on the full MMI design problem (80 x 80 density):
+    forward + adjoint solve + fused gradient kernel, fp32 and fp64."""
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+    from emopt_b200 import adjoint as A
+    from emopt_b200 import problems as P
+    p = P.mmi_gradient(seed=1, nd=(80, 80))
+    res = {}
+    for prec in ("fp32", "fp64"):
+        obj, params = A.mmi_objective(p, prec, device=local)
+        times = []
+        for k in range(args.warmup + args.steps):
+            x = params.clone().requires_grad_(True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            F = obj(x)
+            F.backward()
+            torch.cuda.synchronize()
+            if k >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        res[prec] = {"F": F.item(), "grad": x.grad.detach().cpu().numpy(), "s": statistics.median(times),
+                     "fwd_steps": obj.solver.last["forward"]["steps"],
+                     "adj_steps": obj.solver.last["adjoint"]["steps"],
+                     "fwd_ms": obj.solver.last["forward"]["device_ms"],
+                     "adj_ms": obj.solver.last["adjoint"]["device_ms"]}
+    g32, g64 = res["fp32"]["grad"], res["fp64"]["grad"]
+    cells = p.ncells * (res["fp32"]["fwd_steps"] + res["fp32"]["adj_steps"])
+    result = {
+        "metric": "gradient evaluations/s (forward + adjoint CW solve + overlap, MMI 321x161x101, "
+                  "80x80 density, fp32)",
+        "value": 1.0 / res["fp32"]["s"], "unit": "gradients/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * res["fp32"]["s"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "mmi_grad_321x161x101", "density": [80, 80], "rtol": 1e-6},
+        "gcell_updates_per_s": cells / res["fp32"]["s"] / 1e9,
+        "fp32": {k: v for k, v in res["fp32"].items() if k != "grad"},
+        "fp64": {k: v for k, v in res["fp64"].items() if k != "grad"},
+        "fp32_vs_fp64": {"objective_rel": abs(res["fp32"]["F"] - res["fp64"]["F"]) / abs(res["fp64"]["F"]),
+                         "gradient_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))},
+    }
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "serving":
+        run_serving(args)
+    elif args.workload == "grad":
+        run_grad(args)
     else:
         run_ours(args)
 

@@ -1225,3 +1225,7 @@ extern "C" int FDTD_solve_cw(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolve
     std::memset(res, 0, sizeof(*res));
     return h->precision == 32 ? solve_impl<float>(h, o, res) : solve_impl<double>(h, o, res);
 }
+
+// Continuous batching of CW solves (FDTD_serve_*), in this translation unit
+// so that it shares the resident state and set-up code above.
+#include "serve_engine.cuh"

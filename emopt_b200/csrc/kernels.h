@@ -3,7 +3,7 @@
 
 #include <cuda.h>
 
-#include "grid.cuh"
+#include "cell.cuh"
 
 namespace fdtdb {
 
@@ -136,6 +136,37 @@ struct ProbeDev {
     const long long* map;  // per probe point: offset into the pitched E arrays, or -1
     int nconv;
 };
+
+// ---------------------------------------------------------------- serving
+// Loop state of one request in the batched stepping (serve_kernels.cu).
+enum ServeState { SERVE_FREE = 0, SERVE_RUN = 1, SERVE_TAIL = 2, SERVE_EXTRACT = 3, SERVE_DONE = 4 };
+
+struct ServeCtl {
+    long long n;            // time steps taken
+    long long Tn, last, n0, nprobes;
+    double Nmax, amp_tol, phi_tol, dt, A_change, phi_change;
+    ProbeDev pd;
+    int state, capture, fixed, pad;
+};
+
+template <typename T>
+struct ServeView {
+    GridView<T> g;
+    Fields<T> f;
+    T* snap[2][6];
+    SourceList<T> src;
+    long long nxb;          // 32-vector blocks per row
+};
+
+// Resident single-warp CTAs per SM of the batched step kernels.
+template <typename T>
+int serve_step_ctas_per_sm();
+
+// One time step of every request in the slot tables: H, E, loop events,
+// captures.  Fixed launch shapes (graph-capturable).
+template <typename T>
+cudaError_t launch_serve_step(const ServeView<T>* views, ServeCtl* ctl, const long long* task0,
+                              int nslots, int step_ctas, int copy_ctas, cudaStream_t st);
 
 template <typename T>
 void launch_probe(const T* Ex, const T* Ey, const T* Ez, ProbeDev pd, long long* step_base,

@@ -146,10 +146,29 @@ NOALLOC_MAX_VALUES = 524288
 libFDTD.FDTD_grad_eps.argtypes = [c_int, c_void_p, POINTER(c_void_p), POINTER(c_void_p), c_int,
                                   c_int, c_int, POINTER(c_int), c_int, c_void_p, c_char_p, c_int]
 libFDTD.FDTD_grad_eps.restype = c_int
+libFDTD.FDTD_serve_new.argtypes = [c_int, c_double, c_int, c_int]
+libFDTD.FDTD_serve_new.restype = c_void_p
+libFDTD.FDTD_serve_last_error.argtypes = [c_void_p, c_char_p, c_int]
+libFDTD.FDTD_serve_last_error.restype = c_int
+libFDTD.FDTD_serve_admit.argtypes = [c_void_p, c_void_p, POINTER(SolveOptions)]
+libFDTD.FDTD_serve_admit.restype = c_int
+libFDTD.FDTD_serve_advance.argtypes = [c_void_p]
+libFDTD.FDTD_serve_advance.restype = c_int
+libFDTD.FDTD_serve_finished.argtypes = [c_void_p, POINTER(c_void_p), c_int]
+libFDTD.FDTD_serve_finished.restype = c_int
+libFDTD.FDTD_serve_collect.argtypes = [c_void_p, POINTER(c_void_p), POINTER(SolveResult), c_int]
+libFDTD.FDTD_serve_collect.restype = c_int
+libFDTD.FDTD_serve_info.argtypes = [c_void_p, POINTER(c_double), POINTER(c_int)]
+libFDTD.FDTD_serve_info.restype = c_int
+libFDTD.FDTD_serve_delete.argtypes = [c_void_p]
+libFDTD.FDTD_serve_delete.restype = None
 
 ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_zchunk",
                  "FDTD_set_precision", "FDTD_set_kernel", "FDTD_solve_cw",
-                 "FDTD_amp_phase_noalloc", "FDTD_grad_eps")
+                 "FDTD_amp_phase_noalloc", "FDTD_grad_eps", "FDTD_serve_new",
+                 "FDTD_serve_last_error", "FDTD_serve_admit", "FDTD_serve_advance",
+                 "FDTD_serve_finished", "FDTD_serve_collect", "FDTD_serve_info",
+                 "FDTD_serve_delete")
 
 
 class FDTDError(RuntimeError):

@@ -190,6 +190,50 @@ int FDTD_grad_eps(int device, void *stream, const fdtd_complex128 *const *fwd,
                   const fdtd_complex128 *const *adj, int Nx, int Ny, int Nz, const int *box,
                   int planar, double *out, char *msg, int msglen);
 
+/* ------------------------------------------------------------------ serving
+ * Continuous batching of independent CW solves on one GPU.  No counterpart in
+ * the reference (one solve per process there).  A request is a handle
+ * configured through the calls above (grid, materials, CPML, sources,
+ * FDTD_set_precision(h, 32)) plus its FDTDSolveOptions.  Admitted requests
+ * keep their fields resident and advance together: every FDTD_serve_advance
+ * replays one CUDA graph of steps_per_replay time steps in which batched
+ * kernels step all active requests at once and run each request's probe /
+ * convergence / capture schedule on the device; requests whose loop ended
+ * stop stepping and wait for FDTD_serve_collect, which extracts their fields
+ * into the handle's t0 arrays and frees their memory.  Step counts and fields
+ * equal those of FDTD_solve_cw (vector kernel) for the same request. */
+typedef struct FDTDServe FDTDServe;
+
+/* Engine on `device` with a device-memory budget for the requests' state,
+ * at most max_requests admitted at a time.  Check FDTD_serve_last_error. */
+FDTDServe *FDTD_serve_new(int device, double budget_bytes, int max_requests, int steps_per_replay);
+
+/* Status and message of the engine's last failing call. */
+int FDTD_serve_last_error(FDTDServe *s, char *buf, int buflen);
+
+/* Admit a request: returns its slot (>= 0), -1 when the budget or the slot
+ * table has no room for it now (collect finished requests and retry), or
+ * -(status) on an invalid request.  The handle must not be used elsewhere
+ * until it has been collected. */
+int FDTD_serve_admit(FDTDServe *s, FDTDHandle *h, const FDTDSolveOptions *opt);
+
+/* One graph replay; returns how many requests are ready to collect. */
+int FDTD_serve_advance(FDTDServe *s);
+
+/* Handles of up to max finished, not yet collected requests (so that their
+ * t0 arrays can be provided just before collection); returns the count. */
+int FDTD_serve_finished(FDTDServe *s, FDTDHandle **done, int max);
+
+/* Retire up to max finished requests (fields into their t0 arrays); returns
+ * the count, with the handles in done[] and their results in res[]. */
+int FDTD_serve_collect(FDTDServe *s, FDTDHandle **done, FDTDSolveResult *res, int max);
+
+/* Device bytes held by admitted requests and their number. */
+int FDTD_serve_info(FDTDServe *s, double *used_bytes, int *active);
+
+/* Releases the engine (and the state of requests never collected). */
+void FDTD_serve_delete(FDTDServe *s);
+
 /* Largest n accepted by FDTD_amp_phase_noalloc: 524288 complex128 values, the
  * 8 MiB device array it stages through. */
 #define FDTD_NOALLOC_MAX_VALUES 524288
