@@ -163,10 +163,12 @@ template <typename T>
 int serve_step_ctas_per_sm();
 
 // One time step of every request in the slot tables: H, E, loop events,
-// captures.  Fixed launch shapes (graph-capturable).
+// captures.  Fixed launch shapes (graph-capturable); cap_count is one int of
+// device memory for the per-step capture count.
 template <typename T>
 cudaError_t launch_serve_step(const ServeView<T>* views, ServeCtl* ctl, const long long* task0,
-                              int nslots, int step_ctas, int copy_ctas, cudaStream_t st);
+                              int nslots, long long step_ctas, int copy_ctas, int* cap_count,
+                              cudaStream_t st);
 
 template <typename T>
 void launch_probe(const T* Ex, const T* Ey, const T* Ez, ProbeDev pd, long long* step_base,

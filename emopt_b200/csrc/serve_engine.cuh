@@ -23,6 +23,7 @@ struct FDTDServe {
     fdtdb::ServeView<float>* d_views = nullptr;
     fdtdb::ServeCtl* d_ctl = nullptr;
     long long* d_task0 = nullptr;
+    int* d_cap = nullptr;                      // per-step capture count
     fdtdb::ServeCtl* h_ctl = nullptr;          // pinned mirror
     std::vector<fdtdb::ServeView<float>> views;
     std::vector<long long> task0;
@@ -106,7 +107,7 @@ int serve_capture_graph(FDTDServe* s) {
     cudaError_t e = cudaSuccess;
     for (int q = 0; q < s->L && e == cudaSuccess; q++)
         e = fdtdb::launch_serve_step<float>(s->d_views, s->d_ctl, s->d_task0, s->cap, s->step_ctas,
-                                           s->copy_ctas, s->stream);
+                                           s->copy_ctas, s->d_cap, s->stream);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
     if (e != cudaSuccess) return s->cuda_fail(e, "serve step capture");
@@ -142,6 +143,8 @@ extern "C" FDTDServe* FDTD_serve_new(int device, double budget_bytes, int max_re
     if (e == cudaSuccess) e = cudaMalloc(&s->d_views, sizeof(fdtdb::ServeView<float>) * s->cap);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_ctl, sizeof(fdtdb::ServeCtl) * s->cap);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_task0, sizeof(long long) * (s->cap + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_cap, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_cap, 0, sizeof(int), s->stream);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_ctl, sizeof(fdtdb::ServeCtl) * s->cap);
     if (e != cudaSuccess) {
         s->cuda_fail(e, "FDTD_serve_new");
@@ -158,8 +161,8 @@ extern "C" FDTDServe* FDTD_serve_new(int device, double budget_bytes, int max_re
     e = cudaMemcpyAsync(s->d_ctl, s->h_ctl, sizeof(fdtdb::ServeCtl) * s->cap, cudaMemcpyDefault, s->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->d_views, 0, sizeof(fdtdb::ServeView<float>) * s->cap, s->stream);
     if (e != cudaSuccess) { s->cuda_fail(e, "FDTD_serve_new"); return s; }
-    if (serve_upload_tables(s) != FDTD_OK) return s;
     if (serve_capture_graph(s) != FDTD_OK) return s;
+    if (serve_upload_tables(s) != FDTD_OK) return s;
     s->status = FDTD_OK;
     return s;
 }
@@ -383,6 +386,7 @@ extern "C" void FDTD_serve_delete(FDTDServe* s) {
     if (s->d_views) cudaFree(s->d_views);
     if (s->d_ctl) cudaFree(s->d_ctl);
     if (s->d_task0) cudaFree(s->d_task0);
+    if (s->d_cap) cudaFree(s->d_cap);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
