@@ -52,20 +52,26 @@ def parse_args():
     ap.add_argument("--kernel", default="auto",
                     choices=["auto", "scalar", "fused_plain", "fused_tma", "fused_warp", "vector",
                              "vector16", "stream"])
-    ap.add_argument("--workload", default="mmi", choices=["mmi", "waveguide", "serving", "grad"])
+    ap.add_argument("--workload", default="mmi", choices=["mmi", "waveguide", "serving", "grad", "grating"])
     ap.add_argument("--requests", type=int, default=512, help="serving: requests in the stream")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: mean arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
+    ap.add_argument("--fixed-steps", type=int, default=0,
+                    help="run every solve for this many main steps instead of to rtol "
+                         "(short runs for profiler captures)")
+    ap.add_argument("--request-shape", default="",
+                    help="serving: give every request this grid, 'Nz,Ny,Nx' (d = 0.025 um, "
+                         "wavelength 1.55 um, 20-cell CPML)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the fp64 comparison solve")
     return ap.parse_args()
 
 
-def make_problem(workload: str, seed: int):
+def make_problem(workload: str, seed: int, fixed_steps: int = 0):
     from emopt_b200 import problems as P
     if workload == "mmi":
-        return P.mmi_block(seed=seed)
-    return P.waveguide(fixed_steps=None)
+        return P.mmi_block(seed=seed, fixed_steps=fixed_steps or None)
+    return P.waveguide(fixed_steps=fixed_steps or None)
 
 
 def algorithmic_bytes_per_step(shape, w, word: int) -> int:
@@ -215,7 +221,7 @@ def run_reference(args):
     world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
         return
-    p = make_problem(args.workload, 0)
+    p = make_problem(args.workload, 0, fixed_steps=args.fixed_steps)
     for _ in range(args.warmup):
         cpu_baseline(p, budget_s=2.0)
     vals = [cpu_baseline(p, budget_s=12.0) for _ in range(args.steps)]
@@ -235,7 +241,7 @@ def run_reference(args):
 def run_ours(args):
     world, rank, local = dist_setup(args.gpus)
     from emopt_b200 import problems as P
-    p = make_problem(args.workload, seed=rank)
+    p = make_problem(args.workload, seed=rank, fixed_steps=args.fixed_steps)
     sim = P.make_solver(p, precision=args.precision, kernel=args.kernel, device=local)
     t0 = [sim._Ex_fwd_t0, sim._Ey_fwd_t0, sim._Ez_fwd_t0, sim._Hx_fwd_t0, sim._Hy_fwd_t0,
           sim._Hz_fwd_t0]
@@ -347,11 +353,19 @@ def run_serving(args):
     wavelengths through the continuous-batching engine (FDTD_serve_*)."""
     world, rank, local = dist_setup(args.gpus)
     from emopt_b200 import serving as S
-    specs = S.poisson_stream(args.requests, args.rate, seed=3 + rank)
-    # warm-up: two small requests through a throw-away engine (graph, kernels, allocator)
-    warm = S.ServeEngine(local, 8e9, 8, 32)
-    S.run_stream(S.poisson_stream(2, 1e9, seed=99, shape=(40, 40, 48), w_pml=8), warm, realtime=False)
-    warm.close()
+    kw = {}
+    if args.request_shape:
+        kw = dict(shape=tuple(int(v) for v in args.request_shape.split(",")), d=0.025,
+                  wavelength=1.55, w_pml=20)
+    specs = S.poisson_stream(args.requests, args.rate, seed=3 + rank, **kw)
+    for sp in specs:
+        sp.fixed_steps = args.fixed_steps
+    # warm-up: small requests through a throw-away engine (graph, kernels, allocator)
+    if args.warmup > 0:
+        warm = S.ServeEngine(local, 8e9, 8, 32)
+        S.run_stream(S.poisson_stream(min(args.warmup, 4), 1e9, seed=99, shape=(40, 40, 48), w_pml=8),
+                     warm, realtime=False)
+        warm.close()
     eng = S.ServeEngine(local, args.budget_gb * 1e9, 128, 32)
     barrier(world)
     with ClockSampler(local) as clk:
@@ -365,7 +379,7 @@ def run_serving(args):
     result = {
         "metric": "serving: aggregate Gcell-updates/s with p50/p99 latency (CW-FDTD requests, "
                   "Poisson arrivals, mixed grids 64^3..384x256x128, fp32, rtol=1e-6)",
-        "value": value, "unit": UNIT, "n_gpus": world, "steps": len(steps), "warmup": 2,
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": len(steps), "warmup": min(args.warmup, 4),
         "ms_per_step": 1e3 * makespan / max(len(steps), 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "serving_stream", "requests": args.requests, "rate_per_s": args.rate,
@@ -431,6 +445,61 @@ def run_grad(args):
         print(json.dumps(result), flush=True)
 
 
+def run_grating(args):
+    """Large single solve: the 1201 x 601 x 301 grating slab (217 M cells),
+    float32 and float64 on one GPU, through FDTD_solve_cw with device-built
+    materials and device phasors; reports both rates and the fp32 field
+    error against the fp64 solve."""
+    world, rank, local = dist_setup(args.gpus)
+    import ctypes
+    import torch
+    from emopt_b200 import fdtd_ctypes as ct
+    from emopt_b200 import serving as S
+    spec0 = S.grating_spec()
+    dev = torch.device("cuda", local)
+    mu_ones = torch.ones(spec0.ncells, dtype=torch.complex128, device=dev)
+    out, fields = {}, {}
+    for prec in (32, 64):
+        spec = S.grating_spec(precision=prec)
+        spec.fixed_steps = args.fixed_steps
+        req = S.Request(spec, local, mu_ones)
+        req.set_outputs()
+        res = ct.SolveResult()
+        st = ct.libFDTD.FDTD_solve_cw(req.h, ctypes.byref(req.opt), ctypes.byref(res))
+        if st not in (ct.FDTD_OK, ct.FDTD_NMAX):
+            raise RuntimeError(ct.last_error(req.h))
+        req.release_inputs()
+        w = spec.w_pml
+        alg = algorithmic_bytes_per_step(spec.shape, [w] * 6, prec // 8)
+        step_us = 1e3 * res.device_ms / res.steps
+        out[prec] = {"gcell_updates_per_s": spec.ncells * res.steps / res.device_ms / 1e6,
+                     "steps": res.steps, "n_main": res.n_main, "status": st,
+                     "device_s": res.device_ms / 1e3, "total_s": res.total_ms / 1e3,
+                     "step_us": step_us,
+                     "roofline_frac": alg / (step_us * 1e-6) / 1e9 / measured_peak()[0]}
+        fields[prec] = req.out
+        req.out = None
+        req.close()
+        torch.cuda.empty_cache()
+    num = sum(float(torch.sum(torch.abs(a - b) ** 2)) for a, b in zip(fields[32], fields[64]))
+    den = sum(float(torch.sum(torch.abs(b) ** 2)) for b in fields[64])
+    peak, src = measured_peak()
+    result = {
+        "metric": "Gcell-updates/s (CW-FDTD, fp32 storage, grating slab 1201x601x301, rtol=1e-6)",
+        "value": out[32]["gcell_updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": 1e3 * out[32]["device_s"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "grating_1201x601x301", "cells": spec0.ncells, "rtol": 1e-6,
+                   "fixed_steps": args.fixed_steps},
+        "fp32": out[32], "fp64": out[64],
+        "fp32_rel_l2_vs_fp64": (num / den) ** 0.5,
+        "speedup_fp32_over_fp64": out[32]["gcell_updates_per_s"] / out[64]["gcell_updates_per_s"],
+        "peak_gbs": peak, "peak_source": src,
+    }
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -439,6 +508,8 @@ def main():
         run_serving(args)
     elif args.workload == "grad":
         run_grad(args)
+    elif args.workload == "grating":
+        run_grating(args)
     else:
         run_ours(args)
 

@@ -15,6 +15,7 @@
 // code as the kernels.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -32,6 +33,7 @@ namespace {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    bool owned = true;      // false: a view into another DevBuf (never freed here)
     cudaError_t ensure(size_t n) {
         if (n == 0) n = 16;
         if (p && bytes >= n) return cudaSuccess;
@@ -39,12 +41,20 @@ struct DevBuf {
         cudaError_t e = cudaMalloc(&p, n);
         if (e != cudaSuccess) { p = nullptr; return e; }
         bytes = n;
+        owned = true;
         return cudaSuccess;
     }
+    void view(const DevBuf& base, size_t offset, size_t n) {
+        release();
+        p = static_cast<char*>(base.p) + offset;
+        bytes = n;
+        owned = false;
+    }
     void release() {
-        if (p) cudaFree(p);
+        if (p && owned) cudaFree(p);
         p = nullptr;
         bytes = 0;
+        owned = true;
     }
 };
 
@@ -61,6 +71,7 @@ template <typename T>
 struct Resident {
     int Nx = 0, Ny = 0, Nz = 0, px = 0;
     DevBuf F[2][6];          // fields; set 1 is the second buffer of the fused kernel
+    DevBuf Hall[2];          // the three H components of a set, contiguous (F[s][3..5] view it)
     DevBuf bE[3], aE[3], bH[3];
     bool mu_uniform[3] = {true, true, true};
     double mu_value[3] = {1, 1, 1};
@@ -79,6 +90,7 @@ struct Resident {
 
     void release_all() {
         for (auto& s : F) for (auto& b : s) b.release();
+        for (auto& b : Hall) b.release();
         for (int c = 0; c < 3; c++) { bE[c].release(); aE[c].release(); bH[c].release(); }
         for (auto& s : psi) for (auto& a : s) for (auto& b : a) b.release();
         for (auto& a : tab) for (auto& b : a) b.release();
@@ -799,7 +811,14 @@ int alloc_resident(FDTDHandle* h, Resident<T>& r, bool two_sets) {
     r.Nx = h->Nx; r.Ny = h->Ny; r.Nz = h->Nz; r.px = px;
     size_t cells = (size_t)h->Nz * h->Ny * px;
     for (int s = 0; s < (two_sets ? 2 : 1); s++)
-        for (int c = 0; c < 6; c++) CK(r.F[s][c].ensure(sizeof(T) * cells));
+    {
+        for (int c = 0; c < 3; c++) CK(r.F[s][c].ensure(sizeof(T) * cells));
+        // H in one block, so that one L2 access-policy window can cover it
+        if (!r.Hall[s].p || r.Hall[s].bytes < 3 * sizeof(T) * cells) {
+            CK(r.Hall[s].ensure(3 * sizeof(T) * cells));
+            for (int c = 0; c < 3; c++) r.F[s][3 + c].view(r.Hall[s], c * sizeof(T) * cells, sizeof(T) * cells);
+        }
+    }
     for (int c = 0; c < 3; c++) CK(r.bE[c].ensure(sizeof(T) * cells));
     long long slab[3] = {(long long)h->Nz * h->Ny * (h->w[0] + h->w[1]),
                          (long long)h->Nz * (h->w[2] + h->w[3]) * px,
@@ -926,6 +945,18 @@ int prepare_sources(FDTDHandle* h, Resident<T>& r, fdtdb::SourceList<T>& list) {
                                            coef_arr, coef_s, h->Ny, r.px, dptr<T>(co), h->stream);
             CK(cudaGetLastError());
             d.comp[c] = dptr<T>(co);
+        }
+    }
+    for (int side = 0; side < 2; side++) {
+        int* b = list.box[side];
+        b[0] = b[2] = b[4] = 1 << 30;
+        b[1] = b[3] = b[5] = -1;
+        for (size_t q = 0; q < ns; q++) {
+            const fdtdb::DevSource<T>& d = list.s[q];
+            if (!d.comp[3 * side] && !d.comp[3 * side + 1] && !d.comp[3 * side + 2]) continue;
+            b[0] = std::min(b[0], d.i0); b[1] = std::max(b[1], d.i0 + d.I);
+            b[2] = std::min(b[2], d.j0); b[3] = std::max(b[3], d.j0 + d.J);
+            b[4] = std::min(b[4], d.k0); b[5] = std::max(b[5], d.k0 + d.K);
         }
     }
     return FDTD_OK;

@@ -34,6 +34,10 @@ struct DevSource {
 template <typename T>
 struct SourceList {
     int n;
+    // bounding boxes of the sources that drive E (0: a J component is
+    // non-zero) and H (1: an M component), as i0, i1, j0, j1, k0, k1 (half
+    // open); empty (i0 >= i1) when no source drives that half step
+    int box[2][6];
     DevSource<T> s[kMaxSources];
 };
 

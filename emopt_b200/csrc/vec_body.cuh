@@ -62,6 +62,10 @@ __device__ __forceinline__ void vstore(T* p, const T (&d)[V16<T>::N]) {
 template <typename T>
 __device__ __forceinline__ bool sources_touch(const SourceList<T>& src, int comp_base, int i,
                                               int j0, int j1, int k0, int k1) {
+    // the box of all sources of this half step first: a few comparisons on
+    // kernel parameters reject almost every warp
+    const int* b = src.box[comp_base / 3];
+    if (i < b[0] || i >= b[1] || j1 <= b[2] || j0 >= b[3] || k1 <= b[4] || k0 >= b[5]) return false;
     bool hit = false;
     for (int q = 0; q < src.n; q++) {
         const DevSource<T>& s = src.s[q];

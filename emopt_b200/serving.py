@@ -50,6 +50,8 @@ class RequestSpec:
     src_w0: float = 0.4
     arrival: float = 0.0
     fixed_steps: int = 0
+    src_phase_y: float = 0.0    # linear source phase exp(i src_phase_y y), 1/um
+    precision: int = 32          # storage precision of the solve (32 or 64)
 
     @property
     def ncells(self):
@@ -78,6 +80,34 @@ def random_request(rng, rid, shape=None, d=None, wavelength=None, w_pml=15) -> R
                       c[2] - s[2] / 2, c[2] + s[2] / 2, eps))
     return RequestSpec(rid, tuple(shape), d, wavelength, boxes, w_pml=w_pml,
                        src_k=w_pml + 5, src_yz=(L[1] / 2, L[2] / 2), src_w0=0.4)
+
+
+def grating_spec(seed: int = 4, d: float = 0.02, precision: int = 32) -> RequestSpec:
+    """The large single solve: a grating-coupler-like slab, 24 x 12 x 6 um at
+    d = 0.02 um (1201 x 601 x 301 cells, 217 M), 25-cell CPML: Si substrate
+    (eps 12.25) below z = 1.5 um, a 2 um SiO2 box, a 0.22 um Si layer with 40
+    seeded etch trenches (width uniform 0.1-0.4 um, depth 0.11 um, across y)
+    under SiO2, wavelength 1.55 um; Jy Gaussian sheet (w0 = 2 um) on an
+    x-normal plane, tilted by 10 degrees through the linear phase
+    exp(i k0 n_clad sin(10 deg) y)."""
+    rng = np.random.default_rng(seed)
+    Nx, Ny, Nz = (int(round(24.0 / d)) + 1, int(round(12.0 / d)) + 1, int(round(6.0 / d)) + 1)
+    X, Y, Z = (Nx - 1) * d, (Ny - 1) * d, (Nz - 1) * d
+    big = 1e3
+    z_sub, z_box, t_si = 1.5, 2.0, 0.22
+    z0, z1 = z_sub + z_box, z_sub + z_box + t_si
+    boxes = [(-big, big, -big, big, -big, z_sub, EPS_SI),
+             (-big, big, -big, big, z0, z1, EPS_SI)]
+    centres = np.sort(rng.uniform(6.0, 18.0, 40))
+    for xc in centres:
+        w = rng.uniform(0.1, 0.4)
+        boxes.append((xc - w / 2, xc + w / 2, -big, big, z1 - 0.11, z1 + 1e-9, EPS_SIO2))
+    k0 = 2 * np.pi / 1.55
+    w_pml = 25
+    return RequestSpec(0, (Nz, Ny, Nx), d, 1.55, boxes, w_pml=w_pml, src_k=w_pml + 5,
+                       src_yz=(Y / 2, (z0 + z1) / 2), src_w0=2.0,
+                       src_phase_y=k0 * np.sqrt(EPS_SIO2) * np.sin(np.deg2rad(10.0)),
+                       precision=precision)
 
 
 def poisson_stream(n, rate, seed=3, **kw):
@@ -115,7 +145,7 @@ def eps_arrays(spec: RequestSpec, device) -> list:
 
 
 class Request:
-    """A configured library handle for one spec (float32 storage)."""
+    """A configured library handle for one spec (storage precision from the spec)."""
 
     def __init__(self, spec: RequestSpec, device: int, mu_ones: torch.Tensor):
         self.spec = spec
@@ -140,7 +170,7 @@ class Request:
         lib.FDTD_set_pml_properties(h, 3.0, 0.0, 1.0, 3.0)
         lib.FDTD_build_pml(h)
         lib.FDTD_set_source_properties(h, prm["src_T"], prm["src_min"])
-        lib.FDTD_set_precision(h, 32)
+        lib.FDTD_set_precision(h, spec.precision)
         self.eps = eps_arrays(spec, torch.device("cuda", device))
         torch.cuda.synchronize(device)   # the library reads them on its own stream
         _raw.FDTD_set_mat_arrays(h, *[e.data_ptr() for e in self.eps],
@@ -150,7 +180,8 @@ class Request:
         y = np.arange(Ny) * d
         Zg, Yg = np.meshgrid(z, y, indexing="ij")
         yc, zc = spec.src_yz
-        prof = np.exp(-((Yg - yc) ** 2 + (Zg - zc) ** 2) / spec.src_w0 ** 2)
+        prof = np.exp(-((Yg - yc) ** 2 + (Zg - zc) ** 2) / spec.src_w0 ** 2) * \
+            np.exp(1j * spec.src_phase_y * Yg)
         self.src = [np.zeros(Nz * Ny, dtype=np.complex128) for _ in range(6)]
         self.src[1][:] = prof.ravel()
         lib.FDTD_add_source(h, *self.src, 0, 0, spec.src_k, Nz, Ny, 1, True)

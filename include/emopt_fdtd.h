@@ -156,9 +156,9 @@ typedef struct {
     int status;                /* FDTD_OK, FDTD_NMAX or FDTD_NONFINITE */
 } FDTDSolveResult;
 
-/* Caller arrays (fields, materials, t0/t1 arrays, sources) may live in host
- * memory or in device memory of the handle's device: every copy between them
- * and the library's device buffers lets the CUDA runtime infer the direction.
+/* The material and t0/t1 arrays that FDTD_solve_cw reads and writes may live
+ * in host memory or in device memory of the handle's device (every copy lets
+ * the CUDA runtime infer the direction); source arrays are host memory.
  *
  * Device-resident CW solve: equivalent to FDTD_reset_pml, zeroing the fields
  * and the loop of emopt/fdtd.py:1016-1194 (probe window, norm test, capture of
