@@ -155,6 +155,10 @@ class ClockSampler:
 
 
 def dist_setup(n_gpus: int):
+    """One process per GPU (torchrun env): NCCL when the GPUs are visible,
+    gloo on a CPU-only host (the multi-process tests).  Ranks solve their
+    own seeded replica: no collective on the data path, only the timing
+    reductions below."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -162,30 +166,33 @@ def dist_setup(n_gpus: int):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
     return world, rank, local
+
+
+def _reduce(values: list[float], world: int, op):
+    if world == 1:
+        return values
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(values, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=getattr(dist.ReduceOp, op))
+    return t.tolist()
 
 
 def barrier_max(values: list[float], world: int):
     """Max over ranks of each value (device-timed seconds)."""
-    if world == 1:
-        return values
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor(values, dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return t.tolist()
+    return _reduce(values, world, "MAX")
 
 
 def barrier_sum(values: list[float], world: int):
-    if world == 1:
-        return values
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor(values, dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return t.tolist()
+    """Sum over ranks of each value (cell updates)."""
+    return _reduce(values, world, "SUM")
 
 
 def barrier(world: int):
