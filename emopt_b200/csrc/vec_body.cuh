@@ -93,9 +93,11 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
     const PmlAxis<T>& PX = g.pml[0];
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
-    const int ly = act ? slab_local(PY, j, false) : -1;
-    const int lz = act ? slab_local(PZ, i, true) : -1;
-    const bool xs = act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
+    const int ly = slab_local(PY, j, false);   // same for the whole warp
+    const int lz = slab_local(PZ, i, true);
+    // does any lane of the warp touch an x slab?  (the same for all lanes)
+    const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
+    const bool xs = xw && act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
 
     // ---- every load of the thread first
     T ex[V], ey[V], ez[V], exj[V], ezj[V], exi[V], eyi[V], hx[V], hy[V], hz[V];
@@ -120,6 +122,9 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
         }
     }
 #pragma unroll
+    for (int e = 0; e < V; e++) lxs[e] = -1;
+    if (xw) {
+#pragma unroll
     for (int e = 0; e < V; e++) {
         const int k = k0 + e;
         lxs[e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
@@ -127,6 +132,7 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
             const int s = (i * Ny + j) * PX.wsum + lxs[e];
             px0[e] = ld(PX.psi[0] + s); px1[e] = ld(PX.psi[1] + s);
         }
+    }
     }
     T mx[V], my[V], mz[V];
     const bool mu_arr = g.bHarr[0] != nullptr;
@@ -160,7 +166,7 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
         T Hx = hx[e] + mx[e] * (dEydz - dEzdy);
         T Hy = hy[e] + my[e] * (dEzdx - dExdz);
         T Hz = hz[e] + mz[e] * (dExdy - dEydx);
-        if (lxs[e] >= 0) {
+        if (xw && lxs[e] >= 0) {
             const int l = lxs[e];
             const T kv = ld(PX.kinvH + l), bv = ld(PX.bH + l), cv = ld(PX.cH + l);
             px0[e] = cv * dEydx + bv * px0[e];
@@ -195,12 +201,14 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
         const int s = (lz * Ny + j) * px + k0;
         vecb::vstore<T>(PZ.psi[0] + s, pz0); vecb::vstore<T>(PZ.psi[1] + s, pz1);
     }
+    if (xw) {
 #pragma unroll
-    for (int e = 0; e < V; e++)
-        if (lxs[e] >= 0) {
-            const int s = (i * Ny + j) * PX.wsum + lxs[e];
-            PX.psi[0][s] = px0[e]; PX.psi[1][s] = px1[e];
-        }
+        for (int e = 0; e < V; e++)
+            if (lxs[e] >= 0) {
+                const int s = (i * Ny + j) * PX.wsum + lxs[e];
+                PX.psi[0][s] = px0[e]; PX.psi[1][s] = px1[e];
+            }
+    }
 }
 
 template <typename T>
@@ -217,9 +225,11 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
     const PmlAxis<T>& PX = g.pml[0];
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
-    const int ly = act ? slab_local(PY, j, false) : -1;
-    const int lz = act ? slab_local(PZ, i, true) : -1;
-    const bool xs = act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
+    const int ly = slab_local(PY, j, false);   // same for the whole warp
+    const int lz = slab_local(PZ, i, true);
+    // does any lane of the warp touch an x slab?  (the same for all lanes)
+    const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
+    const bool xs = xw && act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
     const bool lossy = g.aE[0] != nullptr;
 
     // ---- every load of the thread first
@@ -246,6 +256,9 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
         if (lossy) { vecb::vload<T>(ax, g.aE[0] + p); vecb::vload<T>(ay, g.aE[1] + p); vecb::vload<T>(az, g.aE[2] + p); }
     }
 #pragma unroll
+    for (int e = 0; e < V; e++) lxs[e] = -1;
+    if (xw) {
+#pragma unroll
     for (int e = 0; e < V; e++) {
         const int k = k0 + e;
         lxs[e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
@@ -253,6 +266,7 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
             const int s = (i * Ny + j) * PX.wsum + lxs[e];
             px2[e] = ld(PX.psi[2] + s); px3[e] = ld(PX.psi[3] + s);
         }
+    }
     }
     const bool srcb = src.n && vecb::sources_touch<T>(src, 0, i, j, j + 1,
                                                 xb * 32 * V, (xb + 1) * 32 * V);
@@ -295,7 +309,7 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
             Ey = ey[e] + (dHxdz - dHzdx) * by[e];
             Ez = ez[e] + (dHydx - dHxdy) * bz[e];
         }
-        if (lxs[e] >= 0) {
+        if (xw && lxs[e] >= 0) {
             const int l = lxs[e];
             const T kv = ld(PX.kinvE + l), bv = ld(PX.bE + l), cv = ld(PX.cE + l);
             px2[e] = cv * dHydx + bv * px2[e];
@@ -330,12 +344,14 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
         const int s = (lz * Ny + j) * px + k0;
         vecb::vstore<T>(PZ.psi[2] + s, pz2); vecb::vstore<T>(PZ.psi[3] + s, pz3);
     }
+    if (xw) {
 #pragma unroll
-    for (int e = 0; e < V; e++)
-        if (lxs[e] >= 0) {
-            const int s = (i * Ny + j) * PX.wsum + lxs[e];
-            PX.psi[2][s] = px2[e]; PX.psi[3][s] = px3[e];
-        }
+        for (int e = 0; e < V; e++)
+            if (lxs[e] >= 0) {
+                const int s = (i * Ny + j) * PX.wsum + lxs[e];
+                PX.psi[2][s] = px2[e]; PX.psi[3][s] = px3[e];
+            }
+    }
 }
 
 }  // namespace fdtdb

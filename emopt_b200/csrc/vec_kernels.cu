@@ -16,10 +16,17 @@
 
 namespace fdtdb {
 
+// Row of the warp.  With single-warp blocks it is blockIdx.y alone, which the
+// compiler knows to be the same for all lanes: the slab tests derived from it
+// become uniform branches instead of predicated code.
+__device__ __forceinline__ int vec_row() {
+    return VEC_BLOCK_ROWS == 1 ? (int)blockIdx.y : (int)(blockIdx.y * VEC_BLOCK_ROWS + threadIdx.y);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_H_vec(GridView<T> g, Fields<T> f, SourceList<T> src,
                                                       const long long* step_base, int off) {
-    vec_update_H<T>(g, f, src, step_base, off, blockIdx.z, blockIdx.y * VEC_BLOCK_ROWS + threadIdx.y,
+    vec_update_H<T>(g, f, src, step_base, off, blockIdx.z, vec_row(),
                     blockIdx.x, threadIdx.x);
 }
 
@@ -28,7 +35,7 @@ __global__ void __launch_bounds__(256) k_update_H_vec(GridView<T> g, Fields<T> f
 template <typename T>
 __global__ void __launch_bounds__(32 * VEC_BLOCK_ROWS) k_update_E_vec(GridView<T> g, Fields<T> f, SourceList<T> src,
                                                       const long long* step_base, int off) {
-    vec_update_E<T>(g, f, src, step_base, off, blockIdx.z, blockIdx.y * VEC_BLOCK_ROWS + threadIdx.y,
+    vec_update_E<T>(g, f, src, step_base, off, blockIdx.z, vec_row(),
                     blockIdx.x, threadIdx.x);
 }
 
