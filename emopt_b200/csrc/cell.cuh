@@ -187,4 +187,78 @@ __device__ __forceinline__ T h_min_ghost(char bc, T first, T wrap) {
     return wrap;
 }
 
+// ------------------------------------------------------ whole-cell updates
+// The H update of cell (i, j, k) in place, with its E neighbours read from the
+// fields (max-face ghosts from the boundary rule, periodic wrap otherwise) and
+// the magnetic currents of the step g.step_tab[*step_ctr + off].
+template <typename T>
+__device__ __forceinline__ void cell_update_H(const GridView<T>& g, const Fields<T>& f,
+                                              const SourceList<T>& src, const long long* step_ctr,
+                                              int off, int i, int j, int k) {
+    const long long p = (long long)i * g.plane + (long long)j * g.px + k;
+    const T *Ex = f.c[0], *Ey = f.c[1], *Ez = f.c[2];
+    const bool px_ = g.bc[0] != '0' && g.bc[0] != 'E' && g.bc[0] != 'H';
+    const bool py_ = g.bc[1] != '0' && g.bc[1] != 'E' && g.bc[1] != 'H';
+    const bool pz_ = g.bc[2] != '0' && g.bc[2] != 'E' && g.bc[2] != 'H';
+    HIn<T> e;
+    e.ex = Ex[p]; e.ey = Ey[p]; e.ez = Ez[p];
+    if (k + 1 < g.Nx) { e.ey_x = Ey[p + 1]; e.ez_x = Ez[p + 1]; }
+    else if (px_) { e.ey_x = Ey[p - k]; e.ez_x = Ez[p - k]; }
+    else { e.ey_x = T(0); e.ez_x = T(0); }
+    if (j + 1 < g.Ny) { e.ex_y = Ex[p + g.px]; e.ez_y = Ez[p + g.px]; }
+    else if (py_) { long long q = p - (long long)j * g.px; e.ex_y = Ex[q]; e.ez_y = Ez[q]; }
+    else { e.ex_y = T(0); e.ez_y = T(0); }
+    if (i + 1 < g.Nz) { e.ex_z = Ex[p + g.plane]; e.ey_z = Ey[p + g.plane]; }
+    else if (pz_) { long long q = p - (long long)i * g.plane; e.ex_z = Ex[q]; e.ey_z = Ey[q]; }
+    else { e.ex_z = T(0); e.ey_z = T(0); }
+    T hx = f.c[3][p], hy = f.c[4][p], hz = f.c[5][p];
+    h_cell<T>(g, i, j, k, p, e, hx, hy, hz, g.pml[0].psi, g.pml[0].psi, g.pml[1].psi,
+              g.pml[1].psi, g.pml[2].psi, g.pml[2].psi, true);
+    if (src.n) {
+        double4 st = g.step_tab[*step_ctr + off];
+        add_sources<T>(src, i, j, k, 3, T(st.x), T(st.y), hx, hy, hz, false);
+    }
+    f.c[3][p] = hx; f.c[4][p] = hy; f.c[5][p] = hz;
+}
+
+// The E update of cell (i, j, k) in place, with its H neighbours read from the
+// fields (min-face ghosts from the boundary rule, periodic wrap otherwise) and
+// the electric currents of the step.
+template <typename T>
+__device__ __forceinline__ void cell_update_E(const GridView<T>& g, const Fields<T>& f,
+                                              const SourceList<T>& src, const long long* step_ctr,
+                                              int off, int i, int j, int k) {
+    const long long p = (long long)i * g.plane + (long long)j * g.px + k;
+    const T *Hx = f.c[3], *Hy = f.c[4], *Hz = f.c[5];
+    EIn<T> h;
+    h.hx = Hx[p]; h.hy = Hy[p]; h.hz = Hz[p];
+    if (k > 0) { h.hy_x = Hy[p - 1]; h.hz_x = Hz[p - 1]; }
+    else {
+        long long q = p + g.Nx - 1;
+        h.hy_x = h_min_ghost<T>(g.bc[0], h.hy, Hy[q]);
+        h.hz_x = h_min_ghost<T>(g.bc[0], h.hz, Hz[q]);
+    }
+    if (j > 0) { h.hx_y = Hx[p - g.px]; h.hz_y = Hz[p - g.px]; }
+    else {
+        long long q = p + (long long)(g.Ny - 1) * g.px;
+        h.hx_y = h_min_ghost<T>(g.bc[1], h.hx, Hx[q]);
+        h.hz_y = h_min_ghost<T>(g.bc[1], h.hz, Hz[q]);
+    }
+    if (i > 0) { h.hx_z = Hx[p - g.plane]; h.hy_z = Hy[p - g.plane]; }
+    else {
+        long long q = p + (long long)(g.Nz - 1) * g.plane;
+        h.hx_z = h_min_ghost<T>(g.bc[2], h.hx, Hx[q]);
+        h.hy_z = h_min_ghost<T>(g.bc[2], h.hy, Hy[q]);
+    }
+    T ex = f.c[0][p], ey = f.c[1][p], ez = f.c[2][p];
+    T bx, by, bz;
+    e_cell<T>(g, i, j, k, p, h, ex, ey, ez, g.pml[0].psi, g.pml[0].psi, g.pml[1].psi,
+              g.pml[1].psi, g.pml[2].psi, g.pml[2].psi, bx, by, bz);
+    if (src.n) {
+        double4 st = g.step_tab[*step_ctr + off];
+        add_sources<T>(src, i, j, k, 0, T(st.z), T(st.w), ex, ey, ez, true);
+    }
+    f.c[0][p] = ex; f.c[1][p] = ey; f.c[2][p] = ez;
+}
+
 }  // namespace fdtdb

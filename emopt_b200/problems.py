@@ -213,8 +213,12 @@ def design_eps(p: Problem, params: np.ndarray):
 
 def random_box(seed: int, shape=(9, 11, 14), d=0.04, w_pml=(3, 4, 3, 2, 3, 4), bc="000",
                complex_eps=False, fixed_steps: int | None = 120, mu_random=False,
-               n_sources=1, rtol=1e-6) -> Problem:
-    """Small random medium with random complex current boxes (parity sweeps)."""
+               n_sources=1, rtol=1e-6, edge_source=False) -> Problem:
+    """Small random medium with random complex current boxes (parity sweeps).
+
+    ``edge_source``: one more current box over the last 4 x cells of a few rows
+    and planes (drawn after the others), so that sources reach the x-max face.
+    """
     Nz, Ny, Nx = shape
     # lengths half a cell short of (N-1) d so that ceil(L/d)+1 gives back N exactly
     X, Y, Z = (Nx - 1.5) * d, (Ny - 1.5) * d, (Nz - 1.5) * d
@@ -241,6 +245,12 @@ def random_box(seed: int, shape=(9, 11, 14), d=0.04, w_pml=(3, 4, 3, 2, 3, 4), b
         arrays = [rng.standard_normal((I, J, K)) + 1j * rng.standard_normal((I, J, K))
                   for _ in range(6)]
         p.sources.append((arrays, i0, j0, k0))
+    if edge_source:
+        I, J, K = max(1, Nz // 2), max(1, Ny // 2), min(4, Nx)
+        arrays = [rng.standard_normal((I, J, K)) + 1j * rng.standard_normal((I, J, K))
+                  for _ in range(6)]
+        p.sources.append((arrays, int(rng.integers(0, Nz - I + 1)), int(rng.integers(0, Ny - J + 1)),
+                          Nx - K))
     return p
 
 

@@ -26,6 +26,17 @@ BOX_KW = {
     "no_pml": dict(seed=8, shape=(8, 9, 10), w_pml=(0, 0, 0, 0, 0, 0), bc="H0E"),
 }
 
+# Rows that end 1-17 cells past a whole number of 64-cell vector blocks: the
+# last vector block of a row has 1-9 active lanes, and a current box covers
+# the last x cells (the x-max slab and face).
+TAIL_KW = {
+    "tail1": dict(seed=21, shape=(6, 7, 65), bc="000", edge_source=True),
+    "tail8_sym": dict(seed=22, shape=(5, 6, 72), bc="EH0", edge_source=True),
+    "tail16_lossy": dict(seed=23, shape=(5, 6, 80), complex_eps=True, bc="0H0", edge_source=True),
+    "tail1_mu": dict(seed=24, shape=(4, 5, 129), mu_random=True, bc="HEH", edge_source=True),
+    "tail17": dict(seed=25, shape=(5, 6, 81), bc="000", edge_source=True),
+}
+
 
 def cuda_lib_path():
     from emopt_b200 import fdtd_ctypes as ct
@@ -123,6 +134,22 @@ def test_solve_cw_fp64_matches_golden(name, kernel):
     F, info, _ = solve_gpu(p, "fp64", kernel)
     assert info["steps"] == int(g["steps"])
     assert rel_l2(F, g["fields"]) < 1e-11
+
+
+@pytest.mark.parametrize("kernel", ["vector", "scalar"])
+@pytest.mark.parametrize("name", list(TAIL_KW))
+def test_row_tail_matches_golden(name, kernel):
+    g = golden(f"box_{name}.npz")
+    p = P.random_box(**TAIL_KW[name])
+    assert input_digest(p) == str(g["digest"]), "problem generator drifted"
+    F, info, _ = solve_gpu(p, "fp64", kernel)
+    assert info["steps"] == int(g["steps"])
+    assert rel_l2(F, g["fields"]) < 1e-11
+    # the last x cells, where the tail path and the edge source act
+    assert rel_l2(F[..., -4:], g["fields"][..., -4:]) < 1e-11
+    if kernel == "vector":
+        F32, _, _ = solve_gpu(p, "fp32", kernel)
+        assert rel_l2(F32, g["fields"]) < 1e-4
 
 
 @pytest.mark.parametrize("kernel", ["stream", "vector16", "vector", "scalar", "fused_plain", "fused_tma", "fused_warp"])

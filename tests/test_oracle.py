@@ -8,7 +8,7 @@ from helpers import golden, input_digest, oracle_for, rel_l2
 from oracle import driver
 
 GOLDEN_BOXES = ["pec", "sym_EH0", "sym_HEH", "sym_0EE", "lossy", "mu_two_src", "wide_pml",
-                "no_pml"]
+                "no_pml", "tail1", "tail8_sym", "tail16_lossy", "tail1_mu", "tail17"]
 BOX_KW = {
     "pec": dict(seed=1, bc="000"),
     "sym_EH0": dict(seed=2, bc="EH0"),
@@ -18,6 +18,13 @@ BOX_KW = {
     "mu_two_src": dict(seed=6, mu_random=True, n_sources=2, bc="E00"),
     "wide_pml": dict(seed=7, shape=(12, 10, 16), w_pml=(5, 5, 4, 4, 5, 5), bc="000"),
     "no_pml": dict(seed=8, shape=(8, 9, 10), w_pml=(0, 0, 0, 0, 0, 0), bc="H0E"),
+    # rows that end 1-17 cells past a whole number of 64-cell vector blocks,
+    # with a current box over the last x cells
+    "tail1": dict(seed=21, shape=(6, 7, 65), bc="000", edge_source=True),
+    "tail8_sym": dict(seed=22, shape=(5, 6, 72), bc="EH0", edge_source=True),
+    "tail16_lossy": dict(seed=23, shape=(5, 6, 80), complex_eps=True, bc="0H0", edge_source=True),
+    "tail1_mu": dict(seed=24, shape=(4, 5, 129), mu_random=True, bc="HEH", edge_source=True),
+    "tail17": dict(seed=25, shape=(5, 6, 81), bc="000", edge_source=True),
 }
 
 needs_ref = pytest.mark.skipif(not driver.available("ref"),
