@@ -113,7 +113,24 @@ __global__ void __launch_bounds__(256) k_probe(const T* Ex, const T* Ey, const T
     if (threadIdx.x == 0) *step_base = *step_base + advance;
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_slab_sample(const T* Ex, const T* Ey, const T* Ez,
+                                                     const long long* map, int np, double* out) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= np) return;
+    const long long off = map[q];
+    out[q] = off >= 0 ? (double)Ex[off] : 0.0;
+    out[np + q] = off >= 0 ? (double)Ey[off] : 0.0;
+    out[2 * np + q] = off >= 0 ? (double)Ez[off] : 0.0;
+}
+
 }  // namespace
+
+template <typename T>
+void launch_slab_sample(const T* Ex, const T* Ey, const T* Ez, const long long* map, int np,
+                        double* out, cudaStream_t st) {
+    if (np > 0) k_slab_sample<T><<<(np + 255) / 256, 256, 0, st>>>(Ex, Ey, Ez, map, np, out);
+}
 
 template <typename T>
 void launch_material_coeffs(const c128* eps, const c128* mu, int Nx, int Ny, int Nz, int px,
@@ -178,7 +195,9 @@ void launch_probe(const T* Ex, const T* Ey, const T* Ez, ProbeDev pd, long long*
                                        c128*, cudaStream_t);                                    \
     template void launch_snapshot_real<T>(const T*, int, int, int, int, c128*, cudaStream_t);   \
     template void launch_probe<T>(const T*, const T*, const T*, ProbeDev, long long*, int,      \
-                                  long long, double, cudaStream_t);
+                                  long long, double, cudaStream_t);                             \
+    template void launch_slab_sample<T>(const T*, const T*, const T*, const long long*, int,     \
+                                        double*, cudaStream_t);
 INST(float)
 INST(double)
 #undef INST

@@ -87,6 +87,8 @@ struct Resident {
     fdtdb::StepMaps maps[2];
     bool maps_valid = false;
     DevBuf pwin, pA, pphi, ptimes, pout, pmap;
+    int halo = 0;            // planes of halo below and above the fields (z slabs)
+    DevBuf psamp;            // z slab: probe samples of all slabs [3][npoints]
 
     void release_all() {
         for (auto& s : F) for (auto& b : s) b.release();
@@ -102,8 +104,10 @@ struct Resident {
         steptab.release(); stepbase.release(); flag.release(); err.release();
         maps_valid = false;
         pwin.release(); pA.release(); pphi.release(); ptimes.release(); pout.release(); pmap.release();
+        psamp.release();
         coeffs_valid = false;
         Nx = Ny = Nz = px = 0;
+        halo = 0;
     }
 };
 
@@ -139,6 +143,16 @@ struct FDTDHandle {
     int precision = 64;
     int kernel = 0;
     int zchunk = 0;   // planes per CTA of the fused kernels (0: automatic)
+    bool ext_stream = false;   // the stream belongs to the caller (FDTD_set_stream)
+
+    // ---- z slab of a distributed solve (FDTD_slab_*): the handle's grid is
+    // the slab, planes [slab_i0, slab_i0 + Nz) of a grid of slab_Nz planes
+    int slab = 0;
+    int slab_i0 = 0, slab_Nz = 0, slab_lo = 0, slab_hi = 0;
+    int slab_np = 0;                 // probe points of all slabs
+    long long slab_Tn = 0;
+    fdtdb::SourceList<float> slab_src32;
+    fdtdb::SourceList<double> slab_src64;
 
     // ---- padded-layout device mirrors for the per-call entry points
     DevBuf lE[3], lH[3], leps[3], lmu[3];
@@ -179,7 +193,7 @@ struct FDTDHandle {
         }
         cudaError_t e = cudaSetDevice(device);
         if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
-        if (!stream) {
+        if (!stream && !ext_stream) {
             if ((e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess)
                 return cuda_fail(e, "cudaStreamCreate");
             for (auto& v : ev)
@@ -698,7 +712,7 @@ void FDTD_delete(FDTDHandle* h) {
         for (int c = 0; c < 6; c++) { h->lt0[c].release(); h->lt1[c].release(); }
         for (auto& v : h->ev) if (v) cudaEventDestroy(v);
         if (h->pinned) cudaFreeHost(h->pinned);
-        if (h->stream) cudaStreamDestroy(h->stream);
+        if (h->stream && !h->ext_stream) cudaStreamDestroy(h->stream);
     }
     delete h;
 }
@@ -803,20 +817,23 @@ bool build_maps(FDTDHandle* h, Resident<T>& r) {
 }
 
 // Allocates the resident arrays for the current grid and PML widths.
+// halo = 1 (z slabs): the six field arrays get one plane below and one above
+// the slab; the interior starts one plane into each array.
 template <typename T>
-int alloc_resident(FDTDHandle* h, Resident<T>& r, bool two_sets) {
+int alloc_resident(FDTDHandle* h, Resident<T>& r, bool two_sets, int halo = 0) {
     int px = (h->Nx + 31) / 32 * 32;
-    bool same = r.Nx == h->Nx && r.Ny == h->Ny && r.Nz == h->Nz && r.px == px;
+    bool same = r.Nx == h->Nx && r.Ny == h->Ny && r.Nz == h->Nz && r.px == px && r.halo == halo;
     if (!same) r.release_all();
-    r.Nx = h->Nx; r.Ny = h->Ny; r.Nz = h->Nz; r.px = px;
+    r.Nx = h->Nx; r.Ny = h->Ny; r.Nz = h->Nz; r.px = px; r.halo = halo;
     size_t cells = (size_t)h->Nz * h->Ny * px;
+    size_t fcells = (size_t)(h->Nz + 2 * halo) * h->Ny * px;
     for (int s = 0; s < (two_sets ? 2 : 1); s++)
     {
-        for (int c = 0; c < 3; c++) CK(r.F[s][c].ensure(sizeof(T) * cells));
+        for (int c = 0; c < 3; c++) CK(r.F[s][c].ensure(sizeof(T) * fcells));
         // H in one block, so that one L2 access-policy window can cover it
-        if (!r.Hall[s].p || r.Hall[s].bytes < 3 * sizeof(T) * cells) {
-            CK(r.Hall[s].ensure(3 * sizeof(T) * cells));
-            for (int c = 0; c < 3; c++) r.F[s][3 + c].view(r.Hall[s], c * sizeof(T) * cells, sizeof(T) * cells);
+        if (!r.Hall[s].p || r.Hall[s].bytes < 3 * sizeof(T) * fcells) {
+            CK(r.Hall[s].ensure(3 * sizeof(T) * fcells));
+            for (int c = 0; c < 3; c++) r.F[s][3 + c].view(r.Hall[s], c * sizeof(T) * fcells, sizeof(T) * fcells);
         }
     }
     for (int c = 0; c < 3; c++) CK(r.bE[c].ensure(sizeof(T) * cells));
@@ -980,11 +997,13 @@ fdtdb::GridView<T> make_view(FDTDHandle* h, Resident<T>& r, int set) {
         fdtdb::PmlAxis<T>& P = g.pml[a];
         P.w0 = h->w[2 * a]; P.w1 = h->w[2 * a + 1]; P.wsum = P.w0 + P.w1;
         P.edge_max = N[a] - P.w1;
+        P.off = 0;
         for (int q = 0; q < 4; q++) P.psi[q] = dptr<T>(r.psi[set][a][q]);
         P.kinvH = dptr<T>(r.tab[a][0]); P.bH = dptr<T>(r.tab[a][1]);
         P.cH = dptr<T>(r.tab[a][2]); P.kinvE = dptr<T>(r.tab[a][3]);
         P.bE = dptr<T>(r.tab[a][4]); P.cE = dptr<T>(r.tab[a][5]);
     }
+    g.zlo = g.zhi = 0;
     g.step_tab = dptr<double4>(r.steptab);
     return g;
 }
@@ -1013,6 +1032,7 @@ template <typename T>
 int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     if (!h->whole_grid())
         return h->fail(FDTD_ERR_ARG, "FDTD_solve_cw needs the whole grid as the local chunk");
+    if (h->slab) return h->fail(FDTD_ERR_ARG, "the handle is a z slab: it is stepped by FDTD_slab_*");
     if (o->Tn <= 0) return h->fail(FDTD_ERR_ARG, "Tn must be positive");
     if (h->Nx <= 0 || h->Ny <= 0 || h->Nz <= 0) return h->fail(FDTD_ERR_ARG, "empty grid");
     Resident<T>& r = resident<T>(h);
@@ -1093,6 +1113,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     pd.win = dptr<double>(r.pwin); pd.A = dptr<double>(r.pA);
     pd.phi = dptr<double>(r.pphi); pd.times = dptr<double>(r.ptimes);
     pd.out = dptr<double>(r.pout); pd.map = dptr<long long>(r.pmap);
+    pd.samples = nullptr;
     pd.nconv = nconv;
 
     long long* sb = dptr<long long>(r.stepbase);
@@ -1260,3 +1281,6 @@ extern "C" int FDTD_solve_cw(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolve
 // Continuous batching of CW solves (FDTD_serve_*), in this translation unit
 // so that it shares the resident state and set-up code above.
 #include "serve_engine.cuh"
+
+// z slabs of a distributed solve (FDTD_slab_*), sharing the same set-up code.
+#include "slab_engine.cuh"

@@ -46,6 +46,8 @@ template <typename T>
 struct PmlAxis {
     int w0, w1, wsum;      // min width, max width, total
     int edge_max;          // first index of the max slab (strict > for z)
+    int off;               // global index of local coordinate 0 (z slab of a
+                           // distributed solve; 0 otherwise)
     T* psi[4];
     const T* kinvH;        // 1/kappa, b, c for the H update
     const T* bH;
@@ -65,6 +67,10 @@ struct GridView {
     const T* bHarr[3];             // H update: dt/mu per cell (null when uniform)
     T bH[3];                       // uniform dt/mu
     char bc[3];
+    // a neighbouring z slab holds the plane below local index 0 (zlo) or above
+    // Nz - 1 (zhi): the field arrays then have a halo plane there, filled by
+    // the exchange, which is read instead of applying the boundary rule
+    char zlo, zhi;
     PmlAxis<T> pml[3];
     const double4* step_tab;       // per step: (S_H, C_H, S_E, C_E)
 };

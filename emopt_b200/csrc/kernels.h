@@ -18,6 +18,12 @@ template <typename T>
 cudaError_t launch_step_vec(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
                             const long long* step_base, int off, cudaStream_t st);
 
+// One half step (half 0: H, 1: E) of the vector pair: the z slabs of a
+// distributed solve exchange halo planes between the two.
+template <typename T>
+cudaError_t launch_half_vec(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
+                            const long long* step_base, int off, int half, cudaStream_t st);
+
 // H and E half-steps with one 16-byte vector (4 floats / 2 doubles) of x cells
 // per thread over flattened (row, vector) pairs (vec4_kernels.cu).  Requires
 // non-periodic boundaries; returns cudaErrorInvalidValue when the row split
@@ -134,6 +140,7 @@ struct ProbeDev {
     double* times;      // [3]
     double* out;        // [0] A_change, [1] phi_change, [2] probe count
     const long long* map;  // per probe point: offset into the pitched E arrays, or -1
+    const double* samples; // when set: this probe's E values, [3 comps][nconv], instead of map
     int nconv;
 };
 
@@ -173,6 +180,12 @@ cudaError_t launch_serve_step(const ServeView<T>* views, ServeCtl* ctl, const lo
 template <typename T>
 void launch_probe(const T* Ex, const T* Ey, const T* Ez, ProbeDev pd, long long* step_base,
                   int last_off, long long advance, double dt, cudaStream_t st);
+
+// out[c * np + q] = E_c[map[q]] (0 where map[q] < 0): the probe values this
+// z slab holds, summed over the slabs by the caller.
+template <typename T>
+void launch_slab_sample(const T* Ex, const T* Ey, const T* Ez, const long long* map, int np,
+                        double* out, cudaStream_t st);
 
 // ------------------------------------------------ padded (ABI) layout, fp64
 struct LegacyView {

@@ -7,6 +7,8 @@
 // ||phi1 - phi0|| / ||phi0|| (:1137-1138) are reduced with warp shuffles, then
 // across warps in shared memory, into pd.out[0..1]; pd.out[2] counts probes.
 // `nprobe` is the index of the last time step taken (its time is nprobe dt).
+// With pd.samples set the new samples are read from there (the probe values
+// gathered from all slabs of a distributed solve) instead of from E.
 #pragma once
 
 #include "kernels.h"
@@ -42,7 +44,8 @@ __device__ __forceinline__ void probe_block(const T* Ex, const T* Ey, const T* E
         for (int c = 0; c < 3; c++) {
             double* w = pd.win + (long long)c * 3 * pd.nconv;
             double w0 = w[pd.nconv + q], w1 = w[2 * pd.nconv + q];
-            double w2 = off >= 0 ? (double)E[c][off] : 0.0;
+            double w2 = pd.samples ? pd.samples[(long long)c * pd.nconv + q]
+                                   : (off >= 0 ? (double)E[c][off] : 0.0);
             w[q] = w0; w[pd.nconv + q] = w1; w[2 * pd.nconv + q] = w2;
             double f = phase_3t(tt[0], tt[1], tt[2], w0, w1, w2);
             double a = amplitude_3t(tt[0], tt[1], tt[2], w0, w1, w2, f);

@@ -180,7 +180,7 @@ extern "C" int FDTD_serve_admit(FDTDServe* s, FDTDHandle* h, const FDTDSolveOpti
     if (!s || !h || !o) return -FDTD_ERR_ARG;
     if (s->status != FDTD_OK && s->status != FDTD_ERR_ARG) return -s->status;
     auto bad = [&](const char* why) { s->fail(FDTD_ERR_ARG, "FDTD_serve_admit: %s", why); return -FDTD_ERR_ARG; };
-    if (!h->whole_grid()) return bad("the request's handle must hold the whole grid");
+    if (!h->whole_grid() || h->slab) return bad("the request's handle must hold the whole grid");
     for (int a = 0; a < 3; a++)
         if (h->bc[a] != '0' && h->bc[a] != 'E' && h->bc[a] != 'H') return bad("periodic boundaries are not served");
     if (h->precision != 32) return bad("served requests use float32 storage (FDTD_set_precision 32)");

@@ -12,7 +12,10 @@
 // before any dependent instruction; the source test is made once per warp.
 // The source coefficients of the step are g.step_tab[*step_ctr + off].
 // Used by the single-solve kernels (vec_kernels.cu) and the batched serving
-// kernels (serve_kernels.cu).  Requires non-periodic boundaries.
+// kernels (serve_kernels.cu).  Requires non-periodic boundaries.  In a z slab
+// of a distributed solve (g.zlo / g.zhi) the neighbour plane across an inner
+// slab face is read from the halo plane of the field arrays, and the z CPML
+// index is taken at the global plane i + g.pml[2].off.
 #pragma once
 
 #include "cell.cuh"
@@ -94,7 +97,7 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
     const int ly = slab_local(PY, j, false);   // same for the whole warp
-    const int lz = slab_local(PZ, i, true);
+    const int lz = slab_local(PZ, i + PZ.off, true);
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
     const bool xs = xw && act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
@@ -109,7 +112,7 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
     if (act) {
         vecb::vload<T>(ex, f.c[0] + p); vecb::vload<T>(ey, f.c[1] + p); vecb::vload<T>(ez, f.c[2] + p);
         if (j + 1 < Ny) { vecb::vload<T>(exj, f.c[0] + p + px); vecb::vload<T>(ezj, f.c[2] + p + px); }
-        if (i + 1 < Nz) { vecb::vload<T>(exi, f.c[0] + p + Ny * px); vecb::vload<T>(eyi, f.c[1] + p + Ny * px); }
+        if (i + 1 < Nz || g.zhi) { vecb::vload<T>(exi, f.c[0] + p + Ny * px); vecb::vload<T>(eyi, f.c[1] + p + Ny * px); }
         vecb::vload<T>(hx, f.c[3] + p); vecb::vload<T>(hy, f.c[4] + p); vecb::vload<T>(hz, f.c[5] + p);
         if (lane == 31 && k0 + V < g.Nx) { ey_n = ld(f.c[1] + p + V); ez_n = ld(f.c[2] + p + V); }
         if (ly >= 0) {
@@ -226,7 +229,7 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
     const int ly = slab_local(PY, j, false);   // same for the whole warp
-    const int lz = slab_local(PZ, i, true);
+    const int lz = slab_local(PZ, i + PZ.off, true);
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
     const bool xs = xw && act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
@@ -243,7 +246,7 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
         vecb::vload<T>(ex, f.c[0] + p); vecb::vload<T>(ey, f.c[1] + p); vecb::vload<T>(ez, f.c[2] + p);
         vecb::vload<T>(bx, g.bE[0] + p); vecb::vload<T>(by, g.bE[1] + p); vecb::vload<T>(bz, g.bE[2] + p);
         if (j > 0) { vecb::vload<T>(hxj, f.c[3] + p - px); vecb::vload<T>(hzj, f.c[5] + p - px); }
-        if (i > 0) { vecb::vload<T>(hxi, f.c[3] + p - Ny * px); vecb::vload<T>(hyi, f.c[4] + p - Ny * px); }
+        if (i > 0 || g.zlo) { vecb::vload<T>(hxi, f.c[3] + p - Ny * px); vecb::vload<T>(hyi, f.c[4] + p - Ny * px); }
         if (lane == 0 && k0 > 0) { hy_p = ld(f.c[4] + p - 1); hz_p = ld(f.c[5] + p - 1); }
         if (ly >= 0) {
             const int s = (i * PY.wsum + ly) * px + k0;
@@ -284,7 +287,7 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
 #pragma unroll
         for (int e = 0; e < V; e++) { hxj[e] = h_min_ghost<T>(g.bc[1], hx[e], T(0)); hzj[e] = h_min_ghost<T>(g.bc[1], hz[e], T(0)); }
     }
-    if (i == 0) {
+    if (i == 0 && !g.zlo) {
 #pragma unroll
         for (int e = 0; e < V; e++) { hxi[e] = h_min_ghost<T>(g.bc[2], hx[e], T(0)); hyi[e] = h_min_ghost<T>(g.bc[2], hy[e], T(0)); }
     }

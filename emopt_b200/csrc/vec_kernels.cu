@@ -58,6 +58,26 @@ cudaError_t launch_step_vec(const GridView<T>& g, T* const* fields, const Source
     return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_half_vec(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
+                            const long long* step_base, int off, int half, cudaStream_t st) {
+    constexpr int V = vecb::V16<T>::N;
+    Fields<T> f;
+    for (int c = 0; c < 6; c++) f.c[c] = fields[c];
+    const int nvec = (g.Nx + V - 1) / V;
+    dim3 block(32, VEC_BLOCK_ROWS);
+    dim3 grid((nvec + 31) / 32, (g.Ny + VEC_BLOCK_ROWS - 1) / VEC_BLOCK_ROWS, g.Nz);
+    if (half == 0) k_update_H_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
+    else k_update_E_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_half_vec<float>(const GridView<float>&, float* const*,
+                                            const SourceList<float>&, const long long*, int, int,
+                                            cudaStream_t);
+template cudaError_t launch_half_vec<double>(const GridView<double>&, double* const*,
+                                             const SourceList<double>&, const long long*, int, int,
+                                             cudaStream_t);
 template cudaError_t launch_step_vec<float>(const GridView<float>&, float* const*,
                                             const SourceList<float>&, const long long*, int,
                                             cudaStream_t);

@@ -163,12 +163,35 @@ libFDTD.FDTD_serve_info.restype = c_int
 libFDTD.FDTD_serve_delete.argtypes = [c_void_p]
 libFDTD.FDTD_serve_delete.restype = None
 
+# z slabs of a distributed solve (emopt_b200/zslab.py)
+libFDTD.FDTD_set_stream.argtypes = [c_void_p, c_void_p]
+libFDTD.FDTD_set_stream.restype = c_int
+libFDTD.FDTD_slab_set.argtypes = [c_void_p, c_int, c_int, c_int, c_int]
+libFDTD.FDTD_slab_set.restype = c_int
+libFDTD.FDTD_slab_begin.argtypes = [c_void_p, POINTER(SolveOptions),
+                                    ndpointer(np.int64, flags="C_CONTIGUOUS"), c_int]
+libFDTD.FDTD_slab_begin.restype = c_int
+libFDTD.FDTD_slab_step.argtypes = [c_void_p, c_longlong, c_int]
+libFDTD.FDTD_slab_step.restype = c_int
+libFDTD.FDTD_slab_halo.argtypes = [c_void_p, POINTER(c_void_p), POINTER(c_longlong)]
+libFDTD.FDTD_slab_halo.restype = c_int
+libFDTD.FDTD_slab_sample.argtypes = [c_void_p, POINTER(c_void_p)]
+libFDTD.FDTD_slab_sample.restype = c_int
+libFDTD.FDTD_slab_probe.argtypes = [c_void_p, c_longlong, POINTER(c_double), POINTER(c_double)]
+libFDTD.FDTD_slab_probe.restype = c_int
+libFDTD.FDTD_slab_capture.argtypes = [c_void_p, c_int]
+libFDTD.FDTD_slab_capture.restype = c_int
+libFDTD.FDTD_slab_finish.argtypes = [c_void_p, c_longlong, c_longlong]
+libFDTD.FDTD_slab_finish.restype = c_int
+
 ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_zchunk",
                  "FDTD_set_precision", "FDTD_set_kernel", "FDTD_solve_cw",
                  "FDTD_amp_phase_noalloc", "FDTD_grad_eps", "FDTD_serve_new",
                  "FDTD_serve_last_error", "FDTD_serve_admit", "FDTD_serve_advance",
                  "FDTD_serve_finished", "FDTD_serve_collect", "FDTD_serve_info",
-                 "FDTD_serve_delete")
+                 "FDTD_serve_delete", "FDTD_set_stream", "FDTD_slab_set", "FDTD_slab_begin",
+                 "FDTD_slab_step", "FDTD_slab_halo", "FDTD_slab_sample", "FDTD_slab_probe",
+                 "FDTD_slab_capture", "FDTD_slab_finish")
 
 
 class FDTDError(RuntimeError):

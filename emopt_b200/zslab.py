@@ -1,0 +1,375 @@
+"""One CW solve split into z slabs over several GPUs (one process per GPU).
+
+The reference runs a large grid over MPI ranks: PETSc cuts the grid into
+blocks (``emopt/fdtd.py:263-297``, ``dist_method='x'`` gives one block of
+whole planes per rank), and ``GhostComm`` refreshes the one-cell ghost layer
+of every block after each half step (``emopt/fdtd.py:1733-1873``,
+``src/fdtd.cpp:1789-1929``).  Here each rank holds a slab of planes on its GPU
+(``FDTD_slab_*`` in ``include/emopt_fdtd.h``) and exchanges only what the next
+half step reads across a slab face (``src/fdtd.cpp:180`` and ``:508``):
+
+* before the H update, Ex and Ey of the first plane of the slab above;
+* before the E update, Hx and Hy of the last plane of the slab below.
+
+Two planes of ``Ny * px`` words per direction per half step, sent with NCCL
+point-to-point operations on the stream the kernels run on.  The convergence
+test is the reference's multi-rank one (``emopt/fdtd.py:411-413`` and
+``:1119-1145``): every rank picks ``int(nconv / nranks)`` points of its own
+padded local arrays, the values at all points are summed over the ranks (each
+value is held by exactly one rank, so the sum is exact), and every rank runs
+the same probe on the full list, so every rank takes the same decisions.  The
+fields equal those of the single-GPU solve cell for cell.
+
+``LocalLink`` runs several slabs in one process (one GPU or several) with
+device copies instead of NCCL; ``TorchLink`` is the multi-process transport
+over ``torch.distributed``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import fdtd_ctypes as _ct
+from .fdtd import derive_parameters
+from .fdtd_ctypes import libFDTD
+
+
+def ownership(N: int, n: int) -> list[tuple[int, int]]:
+    """(start, count) of the planes of each of ``n`` slabs: the first ``N % n``
+    slabs take one plane more (the split of a PETSc DMDA)."""
+    if n <= 0 or n > N:
+        raise ValueError("cannot split %d planes into %d slabs" % (N, n))
+    out, start = [], 0
+    for r in range(n):
+        c = N // n + (1 if r < N % n else 0)
+        out.append((start, c))
+        start += c
+    return out
+
+
+def probe_cells(Nx: int, Ny: int, Nz: int, ranges, nconv: int) -> np.ndarray:
+    """Global cells read by the convergence probes of a multi-rank run.
+
+    Rank r takes ``arange(0, I*J*K, int(I*J*K / n_pts))`` with
+    ``n_pts = int(nconv / nranks)``, indexed into its padded local E arrays
+    (``emopt/fdtd.py:411-413``).  A point on a face ghost reads the value the
+    ghost exchange leaves there: the adjacent block across a z face, the
+    periodic copy within the block across an x or y face, both with
+    wrap-around at the grid ends (``emopt/fdtd.py:1795-1842``); edge and corner
+    ghosts stay zero (-1 here).  Returns (i*Ny + j)*Nx + k per point, in rank
+    order.
+    """
+    n_pts = int(nconv / len(ranges))
+    if n_pts <= 0:
+        raise ValueError("nconv = %d gives no probe point per rank for %d ranks" % (nconv, len(ranges)))
+    K2, J2 = Nx + 2, Ny + 2
+    cells = []
+    for i0, I in ranges:
+        n = I * Ny * Nx
+        for p in np.arange(0, n, int(n / n_pts)):
+            ip, rem = divmod(int(p), J2 * K2)
+            jp, kp = divmod(rem, K2)
+            ghosts = (ip in (0, I + 1)) + (jp in (0, Ny + 1)) + (kp in (0, Nx + 1))
+            if ghosts > 1:
+                cells.append(-1)
+                continue
+            k = Nx - 1 if kp == 0 else (0 if kp == Nx + 1 else kp - 1)
+            j = Ny - 1 if jp == 0 else (0 if jp == Ny + 1 else jp - 1)
+            i = (i0 + ip - 1) % Nz
+            cells.append((i * Ny + j) * Nx + k)
+    return np.asarray(cells, dtype=np.int64)
+
+
+def _device_tensor(ptr: int, n: int, dtype, device: int):
+    """A torch tensor over ``n`` elements of device memory owned by the library."""
+    import torch
+
+    typestr = {np.float32: "<f4", np.float64: "<f8"}[dtype]
+
+    class _Mem:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False),
+                                    "version": 3, "strides": None}
+
+    return torch.as_tensor(_Mem(), device=torch.device("cuda", device))
+
+
+class CudaSlab:
+    """Planes ``[i0, i0 + I)`` of a CW solve as one resident slab on a GPU.
+
+    ``p`` describes the whole solve like ``emopt_b200.problems.Problem``:
+    X, Y, Z, dx, dy, dz, wavelength, w_pml (cells), bc, complex_eps,
+    src_ramp_time, mats (six global [Nz, Ny, Nx] complex arrays: eps x/y/z,
+    mu x/y/z) and sources [(six arrays [I, J, K], i0, j0, k0)] in global cells.
+    """
+
+    def __init__(self, p, i0: int, I: int, precision: str = "fp32", device: int = 0,
+                 stream: int | None = None):
+        prm = derive_parameters(p.X, p.Y, p.Z, p.dx, p.dy, p.dz, p.wavelength, 1.0,
+                                p.nconv or 10)
+        Nx, Ny, Nz = prm["Nx"], prm["Ny"], prm["Nz"]
+        if not (0 <= i0 and I > 0 and i0 + I <= Nz):
+            raise ValueError("slab [%d, %d) outside %d planes" % (i0, i0 + I, Nz))
+        self.Nx, self.Ny, self.Nz, self.i0, self.I = Nx, Ny, Nz, i0, I
+        self.dt = prm["dt"]
+        self.device = device
+        self.dtype = np.float32 if precision == "fp32" else np.float64
+        h = libFDTD.FDTD_new()
+        self.h = h
+        if libFDTD.FDTD_set_device(h, int(device)) != _ct.FDTD_OK:
+            raise _ct.FDTDError(_ct.last_error(h)[1])
+        libFDTD.FDTD_set_wavelength(h, p.wavelength)
+        libFDTD.FDTD_set_physical_dims(h, prm["X"], prm["Y"], p.dz * (I - 1), p.dx, p.dy, p.dz)
+        libFDTD.FDTD_set_grid_dims(h, Nx, Ny, I)
+        libFDTD.FDTD_set_local_grid(h, 0, 0, 0, Nx, Ny, I)
+        libFDTD.FDTD_set_dt(h, self.dt)
+        self._mats = [np.ascontiguousarray(np.asarray(a)[i0:i0 + I], dtype=np.complex128).ravel()
+                      for a in p.mats]
+        libFDTD.FDTD_set_mat_arrays(h, *self._mats)
+        libFDTD.FDTD_set_complex_eps(h, bool(p.complex_eps))
+        libFDTD.FDTD_set_precision(h, 32 if precision == "fp32" else 64)
+        libFDTD.FDTD_set_kernel(h, 5)
+        libFDTD.FDTD_set_pml_widths(h, *[int(w) for w in p.w_pml])
+        libFDTD.FDTD_set_pml_properties(h, 3.0, 0.0, 1.0, 3.0)
+        libFDTD.FDTD_build_pml(h)
+        src_T = p.src_ramp_time if p.src_ramp_time is not None else prm["src_T"]
+        libFDTD.FDTD_set_source_properties(h, src_T, prm["src_min"])
+        libFDTD.FDTD_set_bc(h, p.bc.encode("ascii"))
+        n = Nx * Ny * I
+        self.t0 = [np.zeros(n, dtype=np.complex128) for _ in range(6)]
+        self._t1 = [np.zeros(n, dtype=np.complex128) for _ in range(6)]
+        libFDTD.FDTD_set_t0_arrays(h, *self.t0)
+        libFDTD.FDTD_set_t1_arrays(h, *self._t1)
+        # sources cropped to the slab, in slab coordinates, converted to
+        # amplitude/phase by the library (emopt/fdtd.py:710-747)
+        self._src = []
+        for arrays, si0, sj0, sk0 in p.sources:
+            sI, sJ, sK = np.asarray(arrays[0]).shape
+            lo, hi = max(si0, i0), min(si0 + sI, i0 + I)
+            if lo >= hi:
+                continue
+            cut = [np.ascontiguousarray(np.asarray(a, dtype=np.complex128)[lo - si0:hi - si0]).ravel().copy()
+                   for a in arrays]
+            self._src.append(cut)
+            libFDTD.FDTD_add_source(h, *cut, lo - i0, sj0, sk0, hi - lo, sJ, sK, True)
+        _ct.check(h, "slab set-up")
+        if libFDTD.FDTD_slab_set(h, i0, Nz, int(i0 > 0), int(i0 + I < Nz)) != _ct.FDTD_OK:
+            raise _ct.FDTDError(_ct.last_error(h)[1])
+        if stream is not None and libFDTD.FDTD_set_stream(h, ctypes.c_void_p(stream)) != _ct.FDTD_OK:
+            raise _ct.FDTDError(_ct.last_error(h)[1])
+        self.has_lo, self.has_hi = i0 > 0, i0 + I < Nz
+        self.halo = None
+        self.samples = None
+
+    def _ok(self, rc, what):
+        if rc != _ct.FDTD_OK:
+            raise _ct.FDTDError("%s: %s" % (what, _ct.last_error(self.h)[1]))
+
+    def begin(self, Tn: int, fixed_steps: int, Nmax: float, cells: np.ndarray):
+        opt = _ct.SolveOptions()
+        opt.Tn = int(Tn)
+        opt.Nmax = float(Nmax)
+        opt.fixed_steps = int(fixed_steps or 0)
+        opt.materials_unchanged = 0
+        cells = np.ascontiguousarray(cells, dtype=np.int64)
+        self._ok(libFDTD.FDTD_slab_begin(self.h, ctypes.byref(opt), cells, len(cells)), "FDTD_slab_begin")
+        ptrs = (ctypes.c_void_p * 8)()
+        pe = ctypes.c_longlong()
+        self._ok(libFDTD.FDTD_slab_halo(self.h, ptrs, ctypes.byref(pe)), "FDTD_slab_halo")
+        t = [_device_tensor(ptrs[q], pe.value, self.dtype, self.device) for q in range(8)]
+        self.halo = {"E_send": t[0:2], "E_recv": t[2:4], "H_send": t[4:6], "H_recv": t[6:8]}
+        sp = ctypes.c_void_p()
+        self._ok(libFDTD.FDTD_slab_sample(self.h, ctypes.byref(sp)), "FDTD_slab_sample")
+        self.samples = _device_tensor(sp.value, 3 * max(len(cells), 1), np.float64, self.device)
+
+    def half_step(self, n: int, half: int):
+        self._ok(libFDTD.FDTD_slab_step(self.h, n, half), "FDTD_slab_step")
+
+    def sample(self):
+        sp = ctypes.c_void_p()
+        self._ok(libFDTD.FDTD_slab_sample(self.h, ctypes.byref(sp)), "FDTD_slab_sample")
+        return self.samples
+
+    def probe(self, n_last: int):
+        A, P = ctypes.c_double(), ctypes.c_double()
+        self._ok(libFDTD.FDTD_slab_probe(self.h, n_last, ctypes.byref(A), ctypes.byref(P)),
+                 "FDTD_slab_probe")
+        return A.value, P.value
+
+    def capture(self, which: int):
+        self._ok(libFDTD.FDTD_slab_capture(self.h, which), "FDTD_slab_capture")
+
+    def finish(self, n0: int, Tn: int):
+        self._ok(libFDTD.FDTD_slab_finish(self.h, n0, Tn), "FDTD_slab_finish")
+        return [a.reshape(self.I, self.Ny, self.Nx) for a in self.t0]
+
+    def close(self):
+        if self.h is not None:
+            libFDTD.FDTD_delete(self.h)
+            self.h = None
+
+
+class LocalLink:
+    """Slabs of one process: halo planes and probe sums move by device copies."""
+
+    def __init__(self, slabs):
+        self.slabs = slabs
+
+    def exchange_E(self):
+        for lo, hi in zip(self.slabs[:-1], self.slabs[1:]):
+            for c in range(2):
+                lo.halo["E_recv"][c].copy_(hi.halo["E_send"][c])
+
+    def exchange_H(self):
+        for lo, hi in zip(self.slabs[:-1], self.slabs[1:]):
+            for c in range(2):
+                hi.halo["H_recv"][c].copy_(lo.halo["H_send"][c])
+
+    def sum_samples(self, tensors):
+        total = tensors[0].clone()
+        for t in tensors[1:]:
+            total += t.to(total.device)
+        for t in tensors:
+            t.copy_(total)
+
+
+class TorchLink:
+    """One slab per process; neighbours are ranks - 1 and + 1 of the default
+    ``torch.distributed`` group (NCCL on GPUs, gloo on CPU tensors)."""
+
+    def __init__(self, slab):
+        import torch.distributed as dist
+        self.dist = dist
+        self.slabs = [slab]
+        self.rank = dist.get_rank()
+        self.size = dist.get_world_size()
+
+    def _swap(self, send, send_to, recv, recv_from):
+        dist = self.dist
+        ops = []
+        if recv_from is not None:
+            ops += [dist.P2POp(dist.irecv, t, recv_from) for t in recv]
+        if send_to is not None:
+            ops += [dist.P2POp(dist.isend, t, send_to) for t in send]
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+
+    def exchange_E(self):
+        s = self.slabs[0]
+        self._swap(s.halo["E_send"], self.rank - 1 if s.has_lo else None,
+                   s.halo["E_recv"], self.rank + 1 if s.has_hi else None)
+
+    def exchange_H(self):
+        s = self.slabs[0]
+        self._swap(s.halo["H_send"], self.rank + 1 if s.has_hi else None,
+                   s.halo["H_recv"], self.rank - 1 if s.has_lo else None)
+
+    def sum_samples(self, tensors):
+        for t in tensors:
+            self.dist.all_reduce(t)
+
+
+@dataclass
+class SlabResult:
+    n_main: int
+    steps: int
+    A_change: float
+    phi_change: float
+    nprobes: int
+    converged: bool
+
+
+def run(slabs, link, Tn: int, rtol: float, Nmax: float, fixed_steps: int | None = None,
+        history: list | None = None) -> SlabResult:
+    """The loop of ``FDTD_solve_cw`` (``emopt/fdtd.py:1016-1194``) over the
+    slabs of this process, with the halo exchange before each half step and
+    the probe on the values of all slabs every Tn steps."""
+    fixed = bool(fixed_steps)
+    last = fixed_steps - 1 if fixed else int(np.floor(Nmax))
+
+    def steps(n, count):
+        for m in range(n, n + count):
+            link.exchange_E()
+            for s in slabs:
+                s.half_step(m, 0)
+            link.exchange_H()
+            for s in slabs:
+                s.half_step(m, 1)
+
+    def probe(n_last):
+        link.sum_samples([s.sample() for s in slabs])
+        vals = [s.probe(n_last) for s in slabs]
+        return vals[0]
+
+    n, Ach, Pch, nprobes = 0, 1.0, 1.0, 0
+    amp_tol, phi_tol = rtol, np.sqrt(rtol)
+
+    def not_converged():
+        if fixed:
+            return True
+        return (Ach > amp_tol or Pch > phi_tol or not np.isfinite(Ach) or not np.isfinite(Pch))
+
+    while not_converged():
+        if n > (last if fixed else Nmax):
+            break
+        if n + Tn - 1 > last:
+            steps(n, last - n + 1)
+            n = last + 1
+            continue
+        steps(n, Tn)
+        Ach, Pch = probe(n + Tn - 1)
+        nprobes += 1
+        if history is not None:
+            history.append((n + Tn - 1, Ach, Pch))
+        n += Tn
+    n0 = n
+    for s in slabs:
+        s.capture(0)
+    steps(n0, Tn)
+    for s in slabs:
+        s.capture(1)
+    steps(n0 + Tn, Tn)
+    converged = fixed or not not_converged()
+    return SlabResult(n_main=n0, steps=n0 + 2 * Tn, A_change=Ach, phi_change=Pch,
+                      nprobes=nprobes, converged=converged)
+
+
+def solve(p, ranges, precision="fp32", devices=None, link=None, rank=None, stream=None):
+    """Solve problem ``p`` split into the slabs ``ranges`` [(i0, I), ...].
+
+    In one process (``rank`` None) every slab is built here, on
+    ``devices[s]`` (default: GPU 0 for all), and linked by device copies.
+    Under ``torch.distributed`` (``rank`` given) this process builds slab
+    ``rank`` only, on ``devices[0]``, and exchanges through ``TorchLink``.
+    Returns (result, {slab index: six complex [I, Ny, Nx] arrays}).
+    """
+    prm = derive_parameters(p.X, p.Y, p.Z, p.dx, p.dy, p.dz, p.wavelength, 1.0, p.nconv or 10)
+    Nx, Ny, Nz = prm["Nx"], prm["Ny"], prm["Nz"]
+    Tn = prm["Tn"]
+    Nmax = p.Nmax if p.Nmax is not None else prm["Nmax"]
+    cells = probe_cells(Nx, Ny, Nz, ranges, p.nconv or 10)
+    mine = list(range(len(ranges))) if rank is None else [rank]
+    devices = devices or [0] * len(ranges)
+    devs = [devices[s] if rank is None else devices[0] for s in mine]
+    if stream is None:
+        # the kernels, the copies or NCCL transfers and the probe sums share
+        # each device's current torch stream, which orders them
+        import torch
+        streams = [torch.cuda.current_stream(d).cuda_stream for d in devs]
+    else:
+        streams = [stream] * len(mine)
+    slabs = [CudaSlab(p, *ranges[s], precision=precision, device=d, stream=st)
+             for s, d, st in zip(mine, devs, streams)]
+    try:
+        for s in slabs:
+            s.begin(Tn, p.fixed_steps, Nmax, cells)
+        if link is None:
+            link = LocalLink(slabs) if rank is None else TorchLink(slabs[0])
+        res = run(slabs, link, Tn, p.rtol, Nmax, p.fixed_steps)
+        fields = {s_idx: sl.finish(res.n_main, Tn) for s_idx, sl in zip(mine, slabs)}
+    finally:
+        for s in slabs:
+            s.close()
+    return res, fields

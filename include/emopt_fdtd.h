@@ -234,6 +234,56 @@ int FDTD_serve_info(FDTDServe *s, double *used_bytes, int *active);
 /* Releases the engine (and the state of requests never collected). */
 void FDTD_serve_delete(FDTDServe *s);
 
+/* ---- z slabs of one CW solve split over GPUs (replaces the reference's
+ * multi-rank run: a PETSc DMDA chunk per MPI rank with the ghost exchange of
+ * GhostComm, emopt/fdtd.py:273-297 and :1733-1873, src/fdtd.cpp:1789-1929).
+ * A slab is a handle whose grid dims are the slab's (Nx, Ny, I planes), with
+ * materials, sources and t0 arrays in slab coordinates and the global CPML
+ * widths.  The caller runs the loop of FDTD_solve_cw and moves one pair of
+ * planes per half step between neighbouring slabs:
+ *     E halo (Ex, Ey plane 0 of the slab above) -> FDTD_slab_step(n, 0)
+ *     H halo (Hx, Hy top plane of the slab below) -> FDTD_slab_step(n, 1)
+ * Fields then equal those of the single-GPU solve on the whole grid. */
+
+/* Launch the handle's work on `stream` (a cudaStream_t of the caller, e.g. the
+ * stream a collective library orders its transfers on) instead of its own. */
+int FDTD_set_stream(FDTDHandle *h, void *stream);
+
+/* The handle holds planes [i0, i0 + Nz) of a grid of Nz_global planes (Nz =
+ * its grid dims); has_lo / has_hi: a slab lies below / above (must match i0). */
+int FDTD_slab_set(FDTDHandle *h, int i0, int Nz_global, int has_lo, int has_hi);
+
+/* Resident set-up of the slab (vector kernel, non-periodic boundaries): uses
+ * o->Tn, o->fixed_steps / o->Nmax (step table) and o->materials_unchanged.
+ * cells[q], q < npoints: the probe points of the whole solve as global cells
+ * (iz * Ny + j) * Nx + k, or -1 for a point that is always zero. */
+int FDTD_slab_begin(FDTDHandle *h, const FDTDSolveOptions *o, const long long *cells, int npoints);
+
+/* Half step of time step n: half 0 updates H, half 1 updates E. */
+int FDTD_slab_step(FDTDHandle *h, long long n, int half);
+
+/* Device addresses of the exchanged planes (plane_elems elements each, in the
+ * slab's precision): ptrs[0..1] Ex, Ey of plane 0 (send down); ptrs[2..3] the
+ * Ex, Ey halo above (receive from the slab above); ptrs[4..5] Hx, Hy of the
+ * top plane (send up); ptrs[6..7] the Hx, Hy halo below (receive from below). */
+int FDTD_slab_halo(FDTDHandle *h, void **ptrs, long long *plane_elems);
+
+/* Writes the probe values this slab holds (3 x npoints doubles, zero for the
+ * points of other slabs) into a device buffer and returns its address; the
+ * caller sums the buffers of all slabs into every slab's buffer. */
+int FDTD_slab_sample(FDTDHandle *h, void **samples);
+
+/* The convergence probe of FDTD_solve_cw (emopt/fdtd.py:1072-1138) on the
+ * summed samples after step n_last; returns the amplitude and phase changes. */
+int FDTD_slab_probe(FDTDHandle *h, long long n_last, double *A_change, double *phi_change);
+
+/* Snapshot of the fields (which 0: t0 sample, 1: t1 sample). */
+int FDTD_slab_capture(FDTDHandle *h, int which);
+
+/* 3-sample extraction with t = n0 dt, (n0 + Tn) dt, (n0 + 2 Tn) dt into the
+ * slab's t0 arrays (src/fdtd.cpp:1346-1443). */
+int FDTD_slab_finish(FDTDHandle *h, long long n0, long long Tn);
+
 /* Largest n accepted by FDTD_amp_phase_noalloc: 524288 complex128 values, the
  * 8 MiB device array it stages through. */
 #define FDTD_NOALLOC_MAX_VALUES 524288

@@ -321,34 +321,22 @@ class OracleFDTD:
         }
 
     # ------------------------------------------------- z-slab multi-instance
-    def run_fixed_slabs(self, n_main: int, nthreads: int, extract=True, time_only_steps=None):
-        """Fixed-step solve over ``nthreads`` z-slabs on as many threads.
-
-        Each slab is one library instance configured with ``set_local_grid``
-        (the reference's MPI chunking, ``emopt/fdtd.py:273-297``); ghost planes
-        are exchanged with the GhostComm rule for a z-only decomposition
-        (x/y faces wrap onto the slab itself, z faces come from the adjacent
-        slab with wrap-around).  ctypes releases the GIL during each call, so the
-        slabs advance in parallel.
-
-        ``time_only_steps``: run that many steps and return the wall time only
-        (CPU-baseline timing); otherwise run ``n_main`` + 2 Tn steps and
-        extract like ``solve`` (without convergence probes).
-        """
-        import time as _time
+    def _slab_machine(self, ranges):
+        """One library instance per slab [(i0, I), ...] and a step function
+        that advances all of them with the ghost exchange of GhostComm for a
+        z-only decomposition (x/y faces wrap onto the slab itself, z faces come
+        from the adjacent slab with wrap-around, emopt/fdtd.py:1733-1873)."""
         lib = self.lib
-        Nz, Ny, Nx = self.Nz, self.Ny, self.Nx
-        P = max(1, min(nthreads, Nz))
-        bounds = np.linspace(0, Nz, P + 1).round().astype(int)
+        Ny, Nx = self.Ny, self.Nx
+        P = len(ranges)
         slabs = []
         keep = []
-        for s in range(P):
-            i0, i1 = int(bounds[s]), int(bounds[s + 1])
-            I, J, K = i1 - i0, Ny, Nx
+        for i0, I in ranges:
+            J, K = Ny, Nx
             npad = (I + 2) * (J + 2) * (K + 2)
             E = [np.zeros(npad) for _ in range(3)]
             H = [np.zeros(npad) for _ in range(3)]
-            mats = [np.ascontiguousarray(a[i0:i1]).ravel() for a in self.eps + self.mu]
+            mats = [np.ascontiguousarray(a[i0:i0 + I]).ravel() for a in self.eps + self.mu]
             t0 = [np.zeros(I * J * K, dtype=np.complex128) for _ in range(6)]
             t1 = [np.zeros(I * J * K, dtype=np.complex128) for _ in range(6)]
             h = lib.FDTD_new()
@@ -360,7 +348,6 @@ class OracleFDTD:
         pool = ThreadPoolExecutor(max_workers=P)
 
         def exchange(fields_key):
-            # x/y periodic faces within each slab, z faces across slabs (wrap)
             views = []
             for sl in slabs:
                 I = sl["I"]
@@ -388,6 +375,115 @@ class OracleFDTD:
             half(lib.FDTD_update_E, n, (n + 0.5) * dt)
             exchange("E")
 
+        return slabs, keep, step, pool
+
+    def solve_slabs(self, ranges, fixed_steps: int | None = None, nconv: int = 10, record=False):
+        """The reference's multi-rank solve over the z slabs ``ranges``.
+
+        Every rank picks int(nconv / nranks) probe points of its own padded
+        local E arrays (emopt/fdtd.py:411-413) and reads them after the ghost
+        exchange; the amplitudes and phases of all ranks are concatenated in
+        rank order before the change norms are taken (:1119-1145)."""
+        lib = self.lib
+        Ny, Nx = self.Ny, self.Nx
+        slabs, keep, step, pool = self._slab_machine([(int(a), int(b)) for a, b in ranges])
+        P = len(slabs)
+        n_pts = int(nconv / P)
+        pts = [np.arange(0, sl["I"] * Ny * Nx, int(sl["I"] * Ny * Nx / n_pts)) for sl in slabs]
+        npt = sum(len(q) for q in pts)
+        Nmax = float(fixed_steps - 1) if fixed_steps is not None else self.Nmax
+        rtol = 1e-300 if fixed_steps is not None else self.rtol
+        dt = self.dt
+        Tn = int(np.int64(self.Ncycle * 3 / 4))
+        win = np.zeros((3, 3, npt))
+        phi0 = np.zeros(npt); phi1 = np.zeros(npt)
+        A0 = np.zeros(npt); A1 = np.zeros(npt)
+        t_0 = t_1 = t_2 = 0
+        A_change = phi_change = 1
+        history = []
+        p = n = 0
+        while (A_change > rtol or phi_change > np.sqrt(rtol) or np.isnan(A_change)
+               or np.isinf(A_change) or np.isnan(phi_change) or np.isinf(phi_change)):
+            if n > Nmax:
+                break
+            step(n)
+            if p == Tn - 1:
+                t_0, t_1, t_2 = t_1, t_2, n * dt
+                phi0[:] = phi1
+                A0[:] = A1
+                q = 0
+                for sl, sp in zip(slabs, pts):
+                    for ci in sp:
+                        phs = amps = 0.0
+                        for c in range(3):
+                            win[c, 0, q] = win[c, 1, q]
+                            win[c, 1, q] = win[c, 2, q]
+                            win[c, 2, q] = sl["E"][c][ci]
+                            f0, f1, f2 = win[c, :, q]
+                            ph = lib.FDTD_calc_phase_3T(t_0, t_1, t_2, f0, f1, f2)
+                            am = lib.FDTD_calc_amplitude_3T(t_0, t_1, t_2, f0, f1, f2, ph)
+                            if am < 0:
+                                am *= -1
+                                ph += pi
+                            phs += ph
+                            amps += am
+                        phi1[q] = phs
+                        A1[q] = amps
+                        q += 1
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    A_change = np.linalg.norm(A1 - A0) / np.linalg.norm(A0)
+                    phi_change = np.linalg.norm(phi1 - phi0) / np.linalg.norm(phi0)
+                if record:
+                    history.append((n, float(A_change), float(phi_change)))
+                p = 0
+            else:
+                p += 1
+            n += 1
+        n0 = n
+        list(pool.map(lambda sl: lib.FDTD_capture_t0_fields(sl["h"]), slabs))
+        for m in range(Tn):
+            step(n0 + m)
+        list(pool.map(lambda sl: lib.FDTD_capture_t1_fields(sl["h"]), slabs))
+        for m in range(Tn):
+            step(n0 + Tn + m)
+        list(pool.map(lambda sl: lib.FDTD_calc_complex_fields_3T(
+            sl["h"], n0 * dt, (n0 + Tn) * dt, (n0 + 2 * Tn) * dt), slabs))
+        pool.shutdown()
+        fields = [np.concatenate([sl["t0"][c].reshape(sl["I"], Ny, Nx) for sl in slabs])
+                  for c in range(6)]
+        return {"fields": fields, "steps": int(n0 + 2 * Tn), "n_main": n0, "Tn": Tn,
+                "A_change": float(A_change), "phi_change": float(phi_change), "history": history}
+
+    def run_fixed_slabs(self, n_main: int, nthreads: int, extract=True, time_only_steps=None,
+                        ranges=None):
+        """Fixed-step solve over ``nthreads`` z-slabs on as many threads.
+
+        Each slab is one library instance configured with ``set_local_grid``
+        (the reference's MPI chunking, ``emopt/fdtd.py:273-297``); ghost planes
+        are exchanged with the GhostComm rule for a z-only decomposition
+        (x/y faces wrap onto the slab itself, z faces come from the adjacent
+        slab with wrap-around).  ctypes releases the GIL during each call, so the
+        slabs advance in parallel.
+
+        ``time_only_steps``: run that many steps and return the wall time only
+        (CPU-baseline timing); otherwise run ``n_main`` + 2 Tn steps and
+        extract like ``solve`` (without convergence probes).  ``ranges``: the
+        slabs as [(i0, I), ...] instead of an even split; the result then also
+        holds each slab's padded E arrays after the last exchange ("E_pad").
+        """
+        import time as _time
+        lib = self.lib
+        Nz, Ny, Nx = self.Nz, self.Ny, self.Nx
+        if ranges is None:
+            P = max(1, min(nthreads, Nz))
+            bounds = np.linspace(0, Nz, P + 1).round().astype(int)
+            ranges_ = [(int(bounds[s]), int(bounds[s + 1] - bounds[s])) for s in range(P)]
+        else:
+            ranges_ = [(int(a), int(b)) for a, b in ranges]
+        slabs, keep, step, pool = self._slab_machine(ranges_)
+        dt = self.dt
+        P = len(slabs)
+
         if time_only_steps is not None:
             t_start = _time.perf_counter()
             for n in range(time_only_steps):
@@ -412,4 +508,7 @@ class OracleFDTD:
         pool.shutdown()
         fields = [np.concatenate([sl["t0"][c].reshape(sl["I"], Ny, Nx) for sl in slabs])
                   for c in range(6)]
-        return {"fields": fields, "steps": n_main + 2 * Tn, "n_main": n_main, "Tn": Tn}
+        out = {"fields": fields, "steps": n_main + 2 * Tn, "n_main": n_main, "Tn": Tn}
+        if ranges is not None:
+            out["E_pad"] = [[a.reshape(sl["I"] + 2, Ny + 2, Nx + 2) for a in sl["E"]] for sl in slabs]
+        return out

@@ -1,0 +1,92 @@
+"""GPU tests of the z-slab solve (FDTD_slab_* through emopt_b200/zslab.py).
+
+All slabs run on one GPU in one process (``LocalLink``: halo planes move by
+device copies on the stream the kernels use), which exercises every kernel
+and exchange path of the multi-GPU solve; the NCCL transport differs only in
+how the same planes travel (``TorchLink``, covered over gloo on the CPU).
+
+* fixed step counts: the fields equal the single-GPU solve of the whole grid
+  bit for bit (fp64 and fp32), for 2 and 3 slabs, with CPML slabs and source
+  boxes across slab faces and symmetric / lossy cases;
+* converging runs: step count and fields of the reference's multi-rank solve
+  (the oracle over the same slabs), fp64 to 1e-11 relative.
+"""
+import numpy as np
+import pytest
+
+from emopt_b200 import problems as P
+from emopt_b200 import zslab
+from helpers import oracle_for, oracle_lib, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "pec3": (dict(seed=31, shape=(9, 7, 12), bc="000", edge_source=True), 3),
+    "sym2": (dict(seed=32, shape=(8, 6, 10), bc="EH0", n_sources=2), 2),
+    "lossy3": (dict(seed=33, shape=(10, 6, 9), complex_eps=True, bc="0HE"), 3),
+    "mu_wide": (dict(seed=34, shape=(16, 9, 70), mu_random=True, bc="000",
+                     w_pml=(5, 5, 4, 4, 6, 5), edge_source=True), 4),
+}
+
+
+def _single(p, precision):
+    sim = P.make_solver(p, precision=precision, kernel="vector")
+    info = sim._solve([sim._Ex_fwd_t0, sim._Ey_fwd_t0, sim._Ez_fwd_t0, sim._Hx_fwd_t0,
+                       sim._Hy_fwd_t0, sim._Hz_fwd_t0],
+                      [sim._Ex_fwd_t1, sim._Ey_fwd_t1, sim._Ez_fwd_t1, sim._Hx_fwd_t1,
+                       sim._Hy_fwd_t1, sim._Hz_fwd_t1], sim._sources)
+    return np.stack([sim._raw(c, False) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")]), info
+
+
+def _slabs(p, nslab, precision):
+    ranges = zslab.ownership(p.shape[0], nslab)
+    res, parts = zslab.solve(p, ranges, precision=precision)
+    F = np.stack([np.concatenate([parts[s][c] for s in range(len(ranges))]) for c in range(6)])
+    return F, res
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name", list(CASES))
+def test_fixed_steps_equal_single_gpu_solve(name, precision):
+    kw, nslab = CASES[name]
+    p = P.random_box(**dict(kw, fixed_steps=150))
+    F1, info = _single(p, precision)
+    F, res = _slabs(p, nslab, precision)
+    assert res.steps == info["steps"] and res.n_main == info["n_main"]
+    assert np.array_equal(F, F1)
+
+
+@pytest.mark.parametrize("name", ["pec3", "sym2", "lossy3"])
+def test_converging_run_matches_reference_multirank(name):
+    kw, nslab = CASES[name]
+    p = P.random_box(**dict(kw, fixed_steps=None, rtol=1e-4))
+    p.Nmax = 3000
+    ranges = zslab.ownership(p.shape[0], nslab)
+    ref = oracle_for(p, oracle_lib()).solve_slabs(ranges, nconv=10)
+    F, res = _slabs(p, nslab, "fp64")
+    assert res.n_main == ref["n_main"] and res.steps == ref["steps"]
+    assert res.A_change == pytest.approx(ref["A_change"], rel=1e-6)
+    assert rel_l2(F, np.stack(ref["fields"])) < 1e-11
+
+
+def test_slab_api_rejects_misuse():
+    from emopt_b200 import fdtd_ctypes as ct
+    lib = ct.libFDTD
+    h = lib.FDTD_new()
+    try:
+        lib.FDTD_set_grid_dims(h, 10, 8, 4)
+        lib.FDTD_set_local_grid(h, 0, 0, 0, 10, 8, 4)
+        # neighbours that do not match the slab's place
+        assert lib.FDTD_slab_set(h, 0, 12, 1, 1) == ct.FDTD_ERR_ARG
+        assert lib.FDTD_slab_set(h, 10, 12, 1, 0) == ct.FDTD_ERR_ARG
+        # stepping before FDTD_slab_begin
+        assert lib.FDTD_slab_step(h, 0, 0) == ct.FDTD_ERR_ARG
+        assert lib.FDTD_slab_set(h, 4, 12, 1, 1) == ct.FDTD_OK
+        # a slab handle is not solved by FDTD_solve_cw
+        import ctypes
+        opt, res = ct.SolveOptions(), ct.SolveResult()
+        opt.Tn = 10
+        opt.fixed_steps = 5
+        assert lib.FDTD_solve_cw(h, ctypes.byref(opt), ctypes.byref(res)) == ct.FDTD_ERR_ARG
+    finally:
+        lib.FDTD_delete(h)
