@@ -52,7 +52,10 @@ def parse_args():
     ap.add_argument("--kernel", default="auto",
                     choices=["auto", "scalar", "fused_plain", "fused_tma", "fused_warp", "vector",
                              "vector16", "stream"])
-    ap.add_argument("--workload", default="mmi", choices=["mmi", "waveguide", "serving", "grad", "grating"])
+    ap.add_argument("--workload", default="mmi",
+                    choices=["mmi", "waveguide", "serving", "grad", "grating", "zslab"])
+    ap.add_argument("--slabs", type=int, default=2,
+                    help="zslab on one process: z slabs on this GPU (under torchrun: one per rank)")
     ap.add_argument("--requests", type=int, default=512, help="serving: requests in the stream")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: mean arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
@@ -507,6 +510,58 @@ def run_grating(args):
         print(json.dumps(result), flush=True)
 
 
+def run_zslab(args):
+    """One MMI-block solve split into z slabs (emopt_b200/zslab.py): under
+    torchrun one slab per rank with the halo planes sent over NCCL, otherwise
+    --slabs slabs on this GPU linked by device copies.  Strong scaling: the
+    grid is fixed, the ranks share it."""
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+    from emopt_b200 import problems as P
+    from emopt_b200 import zslab
+    p = P.mmi_block(fixed_steps=args.fixed_steps or None)
+    nslab = world if world > 1 else max(1, args.slabs)
+    ranges = zslab.ownership(p.shape[0], nslab)
+    torch.cuda.set_device(local)
+    ss = zslab.SlabSet(p, ranges, precision=args.precision, devices=[local],
+                       rank=rank if world > 1 else None)
+    times, res = [], None
+    with ClockSampler(local) as clk:
+        for it in range(args.warmup + args.steps):
+            ss.begin()
+            barrier(world)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = ss.run()
+            e1.record()
+            torch.cuda.synchronize()
+            barrier(world)
+            if it >= args.warmup:
+                times.append(e0.elapsed_time(e1) / 1e3)
+    ss.finish()
+    ss.close()
+    (t,) = barrier_max([statistics.median(times)], world)
+    value = p.ncells * res.steps / t / 1e9
+    result = {
+        "metric": "Gcell-updates/s (CW-FDTD, %s storage, MMI block 321x161x101 split in z slabs, rtol=1e-6)"
+                  % args.precision,
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+        "config": {"workload": "mmi_321x161x101_zslab", "slabs": nslab, "ranges": ranges,
+                   "time_steps_per_solve": res.steps, "n_main": res.n_main,
+                   "transport": "nccl" if world > 1 else "device copies (one GPU)"},
+        "step_us": 1e6 * t / res.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -517,6 +572,8 @@ def main():
         run_grad(args)
     elif args.workload == "grating":
         run_grating(args)
+    elif args.workload == "zslab":
+        run_zslab(args)
     else:
         run_ours(args)
 

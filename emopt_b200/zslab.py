@@ -336,40 +336,74 @@ def run(slabs, link, Tn: int, rtol: float, Nmax: float, fixed_steps: int | None 
                       nprobes=nprobes, converged=converged)
 
 
-def solve(p, ranges, precision="fp32", devices=None, link=None, rank=None, stream=None):
-    """Solve problem ``p`` split into the slabs ``ranges`` [(i0, I), ...].
+class SlabSet:
+    """The slabs of problem ``p`` that this process holds, set up and linked.
 
-    In one process (``rank`` None) every slab is built here, on
-    ``devices[s]`` (default: GPU 0 for all), and linked by device copies.
-    Under ``torch.distributed`` (``rank`` given) this process builds slab
-    ``rank`` only, on ``devices[0]``, and exchanges through ``TorchLink``.
-    Returns (result, {slab index: six complex [I, Ny, Nx] arrays}).
+    In one process (``rank`` None) every slab of ``ranges`` [(i0, I), ...] is
+    built here, on ``devices[s]`` (one device or none: that device, or GPU 0,
+    for all), and linked by device copies.  Under ``torch.distributed`` (``rank`` given) this process
+    builds slab ``rank`` only, on ``devices[0]``, and exchanges through
+    ``TorchLink``.  ``begin()`` resets the fields for a new solve, ``run()``
+    steps it, ``finish()`` extracts {slab index: six complex [I, Ny, Nx] arrays}.
     """
-    prm = derive_parameters(p.X, p.Y, p.Z, p.dx, p.dy, p.dz, p.wavelength, 1.0, p.nconv or 10)
-    Nx, Ny, Nz = prm["Nx"], prm["Ny"], prm["Nz"]
-    Tn = prm["Tn"]
-    Nmax = p.Nmax if p.Nmax is not None else prm["Nmax"]
-    cells = probe_cells(Nx, Ny, Nz, ranges, p.nconv or 10)
-    mine = list(range(len(ranges))) if rank is None else [rank]
-    devices = devices or [0] * len(ranges)
-    devs = [devices[s] if rank is None else devices[0] for s in mine]
-    if stream is None:
-        # the kernels, the copies or NCCL transfers and the probe sums share
-        # each device's current torch stream, which orders them
-        import torch
-        streams = [torch.cuda.current_stream(d).cuda_stream for d in devs]
-    else:
-        streams = [stream] * len(mine)
-    slabs = [CudaSlab(p, *ranges[s], precision=precision, device=d, stream=st)
-             for s, d, st in zip(mine, devs, streams)]
-    try:
-        for s in slabs:
-            s.begin(Tn, p.fixed_steps, Nmax, cells)
-        if link is None:
-            link = LocalLink(slabs) if rank is None else TorchLink(slabs[0])
-        res = run(slabs, link, Tn, p.rtol, Nmax, p.fixed_steps)
-        fields = {s_idx: sl.finish(res.n_main, Tn) for s_idx, sl in zip(mine, slabs)}
-    finally:
-        for s in slabs:
+
+    def __init__(self, p, ranges, precision="fp32", devices=None, link=None, rank=None,
+                 stream=None):
+        prm = derive_parameters(p.X, p.Y, p.Z, p.dx, p.dy, p.dz, p.wavelength, 1.0, p.nconv or 10)
+        Nx, Ny, Nz = prm["Nx"], prm["Ny"], prm["Nz"]
+        self.p = p
+        self.Tn = prm["Tn"]
+        self.Nmax = p.Nmax if p.Nmax is not None else prm["Nmax"]
+        self.cells = probe_cells(Nx, Ny, Nz, ranges, p.nconv or 10)
+        self.mine = list(range(len(ranges))) if rank is None else [rank]
+        devices = list(devices or [0])
+        if rank is None and len(devices) == 1:
+            devices = devices * len(ranges)
+        devs = [devices[s] if rank is None else devices[0] for s in self.mine]
+        if stream is None:
+            # the kernels, the copies or NCCL transfers and the probe sums share
+            # each device's current torch stream, which orders them
+            import torch
+            streams = [torch.cuda.current_stream(d).cuda_stream for d in devs]
+        else:
+            streams = [stream] * len(self.mine)
+        self.slabs = []
+        try:
+            for s, d, st in zip(self.mine, devs, streams):
+                self.slabs.append(CudaSlab(p, *ranges[s], precision=precision, device=d, stream=st))
+        except Exception:
+            self.close()
+            raise
+        self.link = link
+        self.rank = rank
+        self.res = None
+
+    def begin(self):
+        for s in self.slabs:
+            s.begin(self.Tn, self.p.fixed_steps, self.Nmax, self.cells)
+        if self.link is None:
+            self.link = LocalLink(self.slabs) if self.rank is None else TorchLink(self.slabs[0])
+
+    def run(self, history=None) -> SlabResult:
+        self.res = run(self.slabs, self.link, self.Tn, self.p.rtol, self.Nmax, self.p.fixed_steps,
+                       history)
+        return self.res
+
+    def finish(self):
+        return {s_idx: sl.finish(self.res.n_main, self.Tn) for s_idx, sl in zip(self.mine, self.slabs)}
+
+    def close(self):
+        for s in self.slabs:
             s.close()
-    return res, fields
+
+
+def solve(p, ranges, precision="fp32", devices=None, link=None, rank=None, stream=None):
+    """Solve problem ``p`` split into the slabs ``ranges`` (see ``SlabSet``).
+    Returns (result, {slab index: six complex [I, Ny, Nx] arrays})."""
+    ss = SlabSet(p, ranges, precision, devices, link, rank, stream)
+    try:
+        ss.begin()
+        res = ss.run()
+        return res, ss.finish()
+    finally:
+        ss.close()
