@@ -184,6 +184,13 @@ libFDTD.FDTD_slab_capture.restype = c_int
 libFDTD.FDTD_slab_finish.argtypes = [c_void_p, c_longlong, c_longlong]
 libFDTD.FDTD_slab_finish.restype = c_int
 
+# layered rectangle materials (emopt_b200/grid.py)
+libFDTD.FDTD_structured_values.argtypes = [c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                           c_void_p, c_int, c_double, c_double, c_double, c_int,
+                                           c_int, c_int, c_int, c_int, c_int, c_double, c_double,
+                                           c_double, c_void_p, c_char_p, c_int]
+libFDTD.FDTD_structured_values.restype = c_int
+
 ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_zchunk",
                  "FDTD_set_precision", "FDTD_set_kernel", "FDTD_solve_cw",
                  "FDTD_amp_phase_noalloc", "FDTD_grad_eps", "FDTD_serve_new",
@@ -191,7 +198,7 @@ ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_
                  "FDTD_serve_finished", "FDTD_serve_collect", "FDTD_serve_info",
                  "FDTD_serve_delete", "FDTD_set_stream", "FDTD_slab_set", "FDTD_slab_begin",
                  "FDTD_slab_step", "FDTD_slab_halo", "FDTD_slab_sample", "FDTD_slab_probe",
-                 "FDTD_slab_capture", "FDTD_slab_finish")
+                 "FDTD_slab_capture", "FDTD_slab_finish", "FDTD_structured_values")
 
 
 class FDTDError(RuntimeError):

@@ -1,46 +1,254 @@
-"""Minimal material objects implementing the ``Material3D.get_values`` protocol.
+"""Layered rectangle materials for ``emopt_b200.fdtd.FDTD``, evaluated on the GPU.
 
-``FDTD.build`` samples permittivity and permeability through
-``get_values(k1, k2, j1, j2, i1, i2, sx, sy, sz, arr)`` (``emopt/grid.py:762``),
-where ``(sx, sy, sz)`` are the Yee offsets in cells.  The reference's smoothed
-``StructuredMaterial3D`` (polygon overlap in ``src/Grid.cpp``) is outside the
-accelerated path; these classes cover uniform media and voxel arrays.
+The names and semantics follow ``emopt.grid`` (``emopt/grid.py``, backed by
+the reference's ``Grid.so``, ``src/Grid.cpp``): ``Rectangle`` primitives with a
+material value and a priority ``layer`` (lower wins), stacked along z by
+``StructuredMaterial3D.add_primitive(prim, z1, z2)``, and
+``ConstantMaterial3D``.  ``get_values`` returns the Yee-cell averages that the
+reference computes -- area-weighted within a z layer, length-weighted across
+layers -- with one CUDA thread per cell (``FDTD_structured_values``), into a
+numpy array or, with ``device=``, into a torch tensor that stays on the GPU
+(``FDTD.set_material_arrays`` takes either).
+
+Primitives are held by reference as in the reference: moving or resizing a
+rectangle after ``add_primitive`` changes the next ``get_values``; the z
+ranges and the priority order are fixed when the primitive is added
+(``src/Grid.cpp:410-433``, ``:627-733``).  Polygon and Circle primitives of
+``emopt.grid`` are not provided; ``FunctionMaterial3D`` samples an analytic
+``f(x, y, z)`` at the Yee points on the host.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
+from . import fdtd_ctypes as _ct
+from .fdtd_ctypes import libFDTD
 
-class ConstantMaterial3D:
+
+class MaterialPrimitive:
+    """A shape with a material value; ``layer``: lower means higher priority."""
+
+    def __init__(self):
+        self._layer = 1
+
+    @property
+    def layer(self):
+        return self._layer
+
+    @layer.setter
+    def layer(self, newlayer):
+        self._layer = int(newlayer)
+
+    def get_layer(self):
+        return self._layer
+
+    def set_layer(self, layer):
+        self._layer = int(layer)
+
+
+class Rectangle(MaterialPrimitive):
+    """Axis-aligned rectangle centred on (x0, y0) with spans (xspan, yspan)."""
+
+    def __init__(self, x0, y0, xspan, yspan):
+        super().__init__()
+        self._x0, self._y0 = float(x0), float(y0)
+        self._xspan, self._yspan = float(xspan), float(yspan)
+        self._mat = 1.0
+
+    x0 = property(lambda s: s._x0, lambda s, v: setattr(s, "_x0", float(v)))
+    y0 = property(lambda s: s._y0, lambda s, v: setattr(s, "_y0", float(v)))
+    width = property(lambda s: s._xspan, lambda s, v: setattr(s, "_xspan", float(v)))
+    height = property(lambda s: s._yspan, lambda s, v: setattr(s, "_yspan", float(v)))
+    material_value = property(lambda s: s._mat, lambda s, v: setattr(s, "_mat", v))
+
+    def set_material(self, mat):
+        self._mat = mat
+
+    def set_position(self, x0, y0):
+        self._x0, self._y0 = float(x0), float(y0)
+
+    def set_width(self, width):
+        self._xspan = float(width)
+
+    def set_height(self, height):
+        self._yspan = float(height)
+
+    def bounds(self):
+        """xmin, xmax, ymin, ymax (``src/Grid.cpp:203-213``)."""
+        return (self._x0 - self._xspan / 2.0, self._x0 + self._xspan / 2.0,
+                self._y0 - self._yspan / 2.0, self._y0 + self._yspan / 2.0)
+
+    def contains_point(self, x, y):
+        """Strictly inside (``src/Grid.cpp:222-228``)."""
+        hw, hh = self._xspan / 2, self._yspan / 2
+        return (x > self._x0 - hw) and (x < self._x0 + hw) and (y > self._y0 - hh) and (y < self._y0 + hh)
+
+
+def _insert_by_priority(prims, prim):
+    """Before the first primitive of a larger layer (``src/Grid.cpp:410-433``)."""
+    for q, other in enumerate(prims):
+        if prim.layer < other.layer:
+            prims.insert(q, prim)
+            return
+    prims.append(prim)
+
+
+class Material3D:
+    def get_values_in(self, domain, sx=0, sy=0, sz=0, arr=None, squeeze=False, device=None):
+        vals = self.get_values(domain.k.start, domain.k.stop, domain.j.start, domain.j.stop,
+                               domain.i.start, domain.i.stop, sx, sy, sz, arr, device=device)
+        return vals.squeeze() if squeeze else vals
+
+
+class ConstantMaterial3D(Material3D):
     """Uniform material (``emopt/grid.py`` ConstantMaterial3D)."""
 
     def __init__(self, value):
-        self.value = complex(value)
+        self._material_value = value
+
+    material_value = property(lambda s: s._material_value,
+                              lambda s, v: setattr(s, "_material_value", v))
+    value = property(lambda s: complex(s._material_value))
 
     def get_value(self, k, j, i):
-        return self.value
+        return complex(self._material_value)
 
-    def get_values(self, k1, k2, j1, j2, i1, i2, sx=0, sy=0, sz=0, arr=None):
+    def get_values(self, k1, k2, j1, j2, i1, i2, sx=0, sy=0, sz=0, arr=None, reshape=True,
+                   device=None):
         shape = (i2 - i1, j2 - j1, k2 - k1)
-        if arr is None:
-            arr = np.zeros(shape, dtype=np.complex128)
-        arr.reshape(-1)[:] = self.value
-        return arr
+        if device is not None:
+            import torch
+            return torch.full(shape, complex(self._material_value), dtype=torch.complex128,
+                              device=torch.device("cuda", device) if isinstance(device, int) else device)
+        out = np.full(shape, self._material_value, dtype=np.complex128)
+        if arr is not None:
+            np.ravel(arr)[:] = out.ravel()
+            out = arr
+        return out if reshape else np.ravel(out)
 
 
-class FunctionMaterial3D:
-    """Material given by ``f(x, y, z) -> value`` evaluated at the staggered Yee points."""
+class FunctionMaterial3D(Material3D):
+    """Material given by ``f(x, y, z) -> value`` evaluated at the staggered Yee
+    points (host numpy; for analytic media in tests and examples)."""
 
     def __init__(self, f, dx, dy, dz):
         self.f, self.dx, self.dy, self.dz = f, dx, dy, dz
 
-    def get_values(self, k1, k2, j1, j2, i1, i2, sx=0, sy=0, sz=0, arr=None):
+    def get_values(self, k1, k2, j1, j2, i1, i2, sx=0, sy=0, sz=0, arr=None, reshape=True,
+                   device=None):
         z = (np.arange(i1, i2) + sz) * self.dz
         y = (np.arange(j1, j2) + sy) * self.dy
         x = (np.arange(k1, k2) + sx) * self.dx
         Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
         vals = np.asarray(self.f(X, Y, Z), dtype=np.complex128)
+        if device is not None:
+            import torch
+            return torch.as_tensor(vals, device=torch.device("cuda", device) if isinstance(device, int) else device)
         if arr is None:
-            return vals
+            return vals if reshape else vals.ravel()
         arr.reshape(-1)[:] = vals.ravel()
         return arr
+
+
+class StructuredMaterial3D(Material3D):
+    """Rectangles stacked in z layers (``src/Grid.cpp:610-874``)."""
+
+    def __init__(self, X, Y, Z, dx, dy, dz):
+        self._X, self._Y, self._Z = X, Y, Z
+        self._dx, self._dy, self._dz = dx, dy, dz
+        self._zs: list[float] = []              # layer boundaries, ascending
+        self._layers: list[list] = []            # primitives of each layer, by priority
+        self._primitives, self._zmins, self._zmaxs = [], [], []
+
+    primitives = property(lambda s: s._primitives)
+    zmins = property(lambda s: s._zmins)
+    zmaxs = property(lambda s: s._zmaxs)
+
+    def add_primitive(self, prim, z1, z2):
+        """Add ``prim`` over z1 <= z < z2, splitting layers as needed
+        (``src/Grid.cpp:627-733``)."""
+        if not isinstance(prim, Rectangle):
+            raise TypeError("only Rectangle primitives are evaluated on the GPU")
+        self._primitives.append(prim)
+        self._zmins.append(z1)
+        self._zmaxs.append(z2)
+        if z1 >= z2:
+            return          # the reference warns and ignores layers without thickness
+        zs, layers = self._zs, self._layers
+        if not zs:
+            zs += [z1, z2]
+            layers.append([prim])
+            return
+        for z in (z1, z2):
+            ins = None                           # last boundary <= z
+            for q, zq in enumerate(zs):
+                if z >= zq:
+                    ins = q
+            if ins is None:                      # below the stack
+                zs.insert(0, z)
+                layers.insert(0, [])
+            elif ins == len(zs) - 1 and z != zs[ins]:   # above the stack
+                zs.append(z)
+                layers.append([])
+            elif z != zs[ins]:                   # inside layer `ins`: split it
+                copy = []
+                for p in layers[ins]:
+                    _insert_by_priority(copy, p)
+                layers.insert(ins, copy)
+                zs.insert(ins + 1, z)
+        for q in range(len(layers)):
+            if z1 <= zs[q] < z2:
+                _insert_by_priority(layers[q], prim)
+
+    def tables(self):
+        """(zs, layer_start, layer_prims, rects) of the current primitives."""
+        prims = []
+        index = {}
+        start = [0]
+        flat = []
+        for layer in self._layers:
+            for p in layer:
+                if id(p) not in index:
+                    index[id(p)] = len(prims)
+                    prims.append(p)
+                flat.append(index[id(p)])
+            start.append(len(flat))
+        rects = np.zeros((max(len(prims), 1), 6))
+        for q, p in enumerate(prims):
+            m = complex(p.material_value)
+            rects[q] = (*p.bounds(), m.real, m.imag)
+        return (np.asarray(self._zs, dtype=np.float64), np.asarray(start, dtype=np.int32),
+                np.asarray(flat if flat else [0], dtype=np.int32), rects, len(prims))
+
+    def get_values(self, k1, k2, j1, j2, i1, i2, sx=0, sy=0, sz=0, arr=None, reshape=True,
+                   device=None):
+        """Cell values at fractional indices (k + sx, j + sy, i + sz) for
+        k1 <= k < k2, j1 <= j < j2, i1 <= i < i2, shaped [i, j, k].  With
+        ``device`` (a CUDA device index or torch device) the result is a torch
+        tensor on that GPU; otherwise a numpy array (``arr`` if given)."""
+        zs, start, flat, rects, nrects = self.tables()
+        shape = (i2 - i1, j2 - j1, k2 - k1)
+        if device is not None:
+            import torch
+            dev = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
+            out = torch.empty(shape, dtype=torch.complex128, device=dev)
+            ptr, dev_index = out.data_ptr(), dev.index or 0
+            stream = torch.cuda.current_stream(dev).cuda_stream
+        else:
+            out = np.empty(shape, dtype=np.complex128) if arr is None else arr
+            if out.dtype != np.complex128 or not out.flags["C_CONTIGUOUS"] or out.size != np.prod(shape):
+                raise ValueError("arr must be a C-contiguous complex128 array of %d values" % np.prod(shape))
+            ptr, dev_index, stream = out.ctypes.data, 0, None
+        msg = ctypes.create_string_buffer(256)
+        if np.prod(shape) > 0:
+            rc = libFDTD.FDTD_structured_values(
+                dev_index, stream, zs.ctypes.data if len(zs) else None, len(zs), start.ctypes.data,
+                flat.ctypes.data, rects.ctypes.data, nrects, self._dx, self._dy, self._dz,
+                k1, k2, j1, j2, i1, i2, float(sx), float(sy), float(sz), ptr, msg, 256)
+            if rc != _ct.FDTD_OK:
+                raise _ct.FDTDError(msg.value.decode())
+        if device is None and not reshape:
+            return np.ravel(out)
+        return out
