@@ -230,6 +230,7 @@ class FDTD(MaxwellSolver):
             cudart = torch._C._cudart
         except (ImportError, AttributeError):
             return
+        self._cudart = cudart          # kept for __del__, which may run at shutdown
         for a in arrays:
             ptr = a.ctypes.data
             if int(cudart.cudaHostRegister(ptr, a.nbytes, 1)) == 0:   # cudaHostRegisterPortable
@@ -244,9 +245,8 @@ class FDTD(MaxwellSolver):
             self._libfdtd = None
         pinned = getattr(self, "_pinned", [])
         if pinned:
-            import torch
             for ptr, _ in pinned:
-                torch._C._cudart.cudaHostUnregister(ptr)
+                self._cudart.cudaHostUnregister(ptr)
             self._pinned = []
 
     # ------------------------------------------------------------ properties
@@ -678,6 +678,50 @@ class FDTD(MaxwellSolver):
         """Copies of the six material arrays (``emopt/fdtd.py:1669-1692``)."""
         return tuple(np.copy(a) for a in (self._eps_x, self._eps_y, self._eps_z,
                                           self._mu_x, self._mu_y, self._mu_z))
+
+    def calc_ydAx_topology(self, domain, update_mu=False, sig_eps=None, sig_mu=None, del_eps=1.0,
+                           del_mu=1.0, planar=False, lam=0.0):
+        """Topology gradient of ``emopt.experimental.fdtd.FDTD``
+        (``emopt/experimental/fdtd.py:37-158``):
+        ``sig_eps * (lam / n + 2 del_eps Im(E . E_adj))`` over the domain (summed
+        over z when ``planar``), followed for ``update_mu`` by
+        ``sig_mu * (lam / n - 2 del_mu Im(H . H_adj))``; unstaggered t0 arrays,
+        as the reference.  The products run on the GPU (``FDTD_grad_eps``,
+        Kahan-compensated z sums); ``sig_eps`` / ``sig_mu`` None means 1."""
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        box = [domain.k.start, domain.k.stop, domain.j.start, domain.j.stop] + \
+            [domain.i.start, domain.i.stop] * 3
+
+        def overlap(comps):
+            f = [torch.as_tensor(self._raw(c, False)).to(dev) for c in comps]
+            a = [torch.as_tensor(self._raw(c, True)).to(dev) for c in comps]
+            nj, nk = box[3] - box[2], box[1] - box[0]
+            ni = box[5] - box[4]
+            out = torch.empty((3, nj, nk) if planar else (3, ni, nj, nk), dtype=torch.float64, device=dev)
+            ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+            fp = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in f])
+            ap = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in a])
+            msg = ctypes.create_string_buffer(256)
+            st = libFDTD.FDTD_grad_eps(dev.index, torch.cuda.current_stream(dev).cuda_stream, fp, ap,
+                                       self._Nx, self._Ny, self._Nz, (ctypes.c_int * 10)(*box),
+                                       1 if planar else 0, ptr(out), msg, len(msg))
+            if st != _ct.FDTD_OK:
+                raise _ct.FDTDError(msg.value.decode())
+            # 2 Im(adj * fwd) per component, summed over the three components
+            return out.sum(dim=0).cpu().numpy()
+
+        g = overlap(("Ex", "Ey", "Ez"))
+        se = 1.0 if sig_eps is None else sig_eps
+        size = np.size(se) if sig_eps is not None else g.size
+        grad_eps = se * (lam / size + del_eps * g)
+        if not update_mu:
+            return np.ravel(grad_eps)
+        gh = overlap(("Hx", "Hy", "Hz"))
+        sm = 1.0 if sig_mu is None else sig_mu
+        size = np.size(sm) if sig_mu is not None else gh.size
+        grad_mu = sm * (lam / size - del_mu * gh)
+        return np.concatenate([np.ravel(grad_eps), np.ravel(grad_mu)])
 
     def calc_ydAx(self, Adiag0):
         """y^T dA x with dA = i (eps - eps0) for E and -i (mu - mu0) for H

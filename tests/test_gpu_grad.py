@@ -112,3 +112,38 @@ def test_grad_eps_kernel_against_torch():
         blk = lambda a: a[i0:i1, d.j0:d.j1, d.k0:d.k1]
         ref = (2 * torch.imag(blk(s.adj[c]) * blk(s.fwd[c]))).sum(0)
         torch.testing.assert_close(got[c], ref, rtol=1e-12, atol=1e-12 * float(ref.abs().max()))
+
+
+@pytest.mark.parametrize("planar", [True, False])
+def test_calc_ydAx_topology_matches_reference_formula(planar):
+    """FDTD.calc_ydAx_topology (products on the GPU) against the numpy lines of
+    emopt/experimental/fdtd.py:121-158 on the same forward/adjoint fields."""
+    from emopt_b200 import problems as P
+    from emopt_b200.misc import DomainCoordinates
+    p = P.random_box(seed=41, shape=(10, 9, 12), fixed_steps=200)
+    sim = P.make_solver(p, precision="fp64")
+    sim.solve_forward()
+    rng = np.random.default_rng(3)
+    I, J, K = 2, 3, 4
+    src = [rng.standard_normal((I, J, K)) + 1j * rng.standard_normal((I, J, K)) for _ in range(6)]
+    dom = DomainCoordinates.from_indices(5, 5 + K, 3, 3 + J, 4, 4 + I, p.dx, p.dy, p.dz)
+    sim.add_adjoint_sources(tuple(src), dom)
+    sim.solve_adjoint()
+    design = DomainCoordinates.from_indices(2, 10, 1, 8, 3, 8, p.dx, p.dy, p.dz)
+    E = [sim.get_field(c, design) for c in ("Ex", "Ey", "Ez")]
+    Ea = [sim.get_adjoint_field(c, design) for c in ("Ex", "Ey", "Ez")]
+    H = [sim.get_field(c, design) for c in ("Hx", "Hy", "Hz")]
+    Ha = [sim.get_adjoint_field(c, design) for c in ("Hx", "Hy", "Hz")]
+    shape = E[0].shape[1:] if planar else E[0].shape
+    sig_e = rng.uniform(0.1, 1.0, shape)
+    sig_m = rng.uniform(0.1, 1.0, shape)
+    de, dm, lam = 10.165, 0.7, 0.01
+    pe = E[0] * Ea[0] + E[1] * Ea[1] + E[2] * Ea[2]
+    ph = H[0] * Ha[0] + H[1] * Ha[1] + H[2] * Ha[2]
+    if planar:
+        pe, ph = np.sum(pe, axis=0), np.sum(ph, axis=0)
+    want = np.concatenate([np.ravel(sig_e * (lam / sig_e.size + 2 * de * np.imag(pe))),
+                           np.ravel(sig_m * (lam / sig_m.size - 2 * dm * np.imag(ph)))])
+    got = sim.calc_ydAx_topology(design, True, sig_e, sig_m, de, dm, planar, lam)
+    assert got.shape == want.shape
+    assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
