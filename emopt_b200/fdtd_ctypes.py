@@ -184,11 +184,12 @@ libFDTD.FDTD_slab_capture.restype = c_int
 libFDTD.FDTD_slab_finish.argtypes = [c_void_p, c_longlong, c_longlong]
 libFDTD.FDTD_slab_finish.restype = c_int
 
-# layered rectangle materials (emopt_b200/grid.py)
+# layered materials (emopt_b200/grid.py)
 libFDTD.FDTD_structured_values.argtypes = [c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
-                                           c_void_p, c_int, c_double, c_double, c_double, c_int,
-                                           c_int, c_int, c_int, c_int, c_int, c_double, c_double,
-                                           c_double, c_void_p, c_char_p, c_int]
+                                           c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p,
+                                           c_int, c_double, c_double, c_double, c_int, c_int, c_int,
+                                           c_int, c_int, c_int, c_double, c_double, c_double,
+                                           c_void_p, c_char_p, c_int]
 libFDTD.FDTD_structured_values.restype = c_int
 
 ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_zchunk",

@@ -1,8 +1,9 @@
-"""Layered rectangle materials for ``emopt_b200.fdtd.FDTD``, evaluated on the GPU.
+"""Layered rectangle and polygon materials for ``emopt_b200.fdtd.FDTD``, evaluated on the GPU.
 
 The names and semantics follow ``emopt.grid`` (``emopt/grid.py``, backed by
 the reference's ``Grid.so``, ``src/Grid.cpp``): ``Rectangle`` primitives with a
-material value and a priority ``layer`` (lower wins), stacked along z by
+material value and a priority ``layer`` (lower wins), and ``Polygon``
+primitives, stacked along z by
 ``StructuredMaterial3D.add_primitive(prim, z1, z2)``, and
 ``ConstantMaterial3D``.  ``get_values`` returns the Yee-cell averages that the
 reference computes -- area-weighted within a z layer, length-weighted across
@@ -13,9 +14,11 @@ numpy array or, with ``device=``, into a torch tensor that stays on the GPU
 Primitives are held by reference as in the reference: moving or resizing a
 rectangle after ``add_primitive`` changes the next ``get_values``; the z
 ranges and the priority order are fixed when the primitive is added
-(``src/Grid.cpp:410-433``, ``:627-733``).  Polygon and Circle primitives of
-``emopt.grid`` are not provided; ``FunctionMaterial3D`` samples an analytic
-``f(x, y, z)`` at the Yee points on the host.
+(``src/Grid.cpp:410-433``, ``:627-733``).  ``Polygon`` primitives are simple
+polygons (convex ones evaluated whole, others through a triangulation made
+here); the reference's ``Circle`` (whose overlap is a stub returning 0) is not
+provided; ``FunctionMaterial3D`` samples an analytic ``f(x, y, z)`` at the
+Yee points on the host.
 """
 from __future__ import annotations
 
@@ -84,6 +87,109 @@ class Rectangle(MaterialPrimitive):
         """Strictly inside (``src/Grid.cpp:222-228``)."""
         hw, hh = self._xspan / 2, self._yspan / 2
         return (x > self._x0 - hw) and (x < self._x0 + hw) and (y > self._y0 - hh) and (y < self._y0 + hh)
+
+
+class Polygon(MaterialPrimitive):
+    """Simple polygon given by its vertices (``emopt/grid.py`` Polygon; a
+    repeated closing vertex is accepted).  Convex polygons are evaluated as
+    one part, others as the triangles of an ear-clipping triangulation."""
+
+    def __init__(self, xs=None, ys=None):
+        super().__init__()
+        self._xs = np.zeros(0)
+        self._ys = np.zeros(0)
+        self._value = 1.0
+        if xs is not None and ys is not None:
+            self.set_points(xs, ys)
+
+    xs = property(lambda s: np.copy(s._xs))
+    ys = property(lambda s: np.copy(s._ys))
+    Np = property(lambda s: len(s._xs))
+    material_value = property(lambda s: s._value, lambda s, v: setattr(s, "_value", v))
+
+    def set_material(self, mat):
+        self._value = mat
+
+    def set_points(self, x, y):
+        self._xs = np.array(x, dtype=np.float64).ravel()
+        self._ys = np.array(y, dtype=np.float64).ravel()
+
+    def add_point(self, x, y):
+        self._xs = np.append(self._xs, float(x))
+        self._ys = np.append(self._ys, float(y))
+
+    def add_points(self, x, y):
+        self._xs = np.concatenate([self._xs, np.asarray(x, dtype=np.float64).ravel()])
+        self._ys = np.concatenate([self._ys, np.asarray(y, dtype=np.float64).ravel()])
+
+    def set_point(self, index, x, y):
+        self._xs[index] = x
+        self._ys[index] = y
+
+    def outline(self):
+        """Vertices counter-clockwise, without a repeated closing vertex."""
+        x, y = self._xs, self._ys
+        if len(x) > 1 and x[0] == x[-1] and y[0] == y[-1]:
+            x, y = x[:-1], y[:-1]
+        if len(x) < 3:
+            raise ValueError("a Polygon needs at least 3 vertices")
+        area2 = np.sum(x * np.roll(y, -1) - np.roll(x, -1) * y)
+        if area2 < 0:
+            x, y = x[::-1], y[::-1]
+        return np.stack([x, y], axis=1)
+
+    def contains_point(self, x, y):
+        v = self.outline()
+        inside = False
+        for q in range(len(v)):
+            (ax, ay), (bx, by) = v[q], v[(q + 1) % len(v)]
+            if (bx - ax) * (y - ay) - (by - ay) * (x - ax) == 0 and min(ax, bx) <= x <= max(ax, bx) \
+                    and min(ay, by) <= y <= max(ay, by):
+                return False
+            if (ay > y) != (by > y) and x < (bx - ax) * (y - ay) / (by - ay) + ax:
+                inside = not inside
+        return inside
+
+
+def _convex_parts(v):
+    """Convex pieces of the counter-clockwise outline v: itself when convex,
+    else the triangles of an ear-clipping triangulation."""
+    n = len(v)
+    cross = [(v[(q + 1) % n][0] - v[q][0]) * (v[(q + 2) % n][1] - v[(q + 1) % n][1]) -
+             (v[(q + 1) % n][1] - v[q][1]) * (v[(q + 2) % n][0] - v[(q + 1) % n][0]) for q in range(n)]
+    if all(c >= 0 for c in cross):
+        return [v]
+    idx = list(range(n))
+    tris = []
+
+    def cr(a, b, c):
+        return (b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0])
+
+    guard = 0
+    while len(idx) > 3 and guard < 10 * n * n:
+        guard += 1
+        m = len(idx)
+        for q in range(m):
+            a, b, c = v[idx[q - 1]], v[idx[q]], v[idx[(q + 1) % m]]
+            if cr(a, b, c) <= 0:
+                continue            # reflex or degenerate corner
+            if any(cr(a, b, v[r]) >= 0 and cr(b, c, v[r]) >= 0 and cr(c, a, v[r]) >= 0
+                   for r in idx if r not in (idx[q - 1], idx[q], idx[(q + 1) % m])):
+                continue            # another vertex inside the ear
+            tris.append(np.array([a, b, c]))
+            del idx[q]
+            break
+        else:
+            raise ValueError("polygon could not be triangulated (is it simple?)")
+    tris.append(np.array([v[r] for r in idx]))
+
+    def area(p):
+        p = np.asarray(p)
+        return 0.5 * abs(np.sum(p[:, 0] * np.roll(p[:, 1], -1) - np.roll(p[:, 0], -1) * p[:, 1]))
+
+    if abs(sum(area(t) for t in tris) - area(v)) > 1e-9 * max(area(v), 1e-300):
+        raise ValueError("polygon edges cross each other: only simple polygons are supported")
+    return tris
 
 
 def _insert_by_priority(prims, prim):
@@ -169,8 +275,8 @@ class StructuredMaterial3D(Material3D):
     def add_primitive(self, prim, z1, z2):
         """Add ``prim`` over z1 <= z < z2, splitting layers as needed
         (``src/Grid.cpp:627-733``)."""
-        if not isinstance(prim, Rectangle):
-            raise TypeError("only Rectangle primitives are evaluated on the GPU")
+        if not isinstance(prim, (Rectangle, Polygon)):
+            raise TypeError("Rectangle and Polygon primitives are evaluated on the GPU")
         self._primitives.append(prim)
         self._zmins.append(z1)
         self._zmaxs.append(z2)
@@ -203,11 +309,10 @@ class StructuredMaterial3D(Material3D):
                 _insert_by_priority(layers[q], prim)
 
     def tables(self):
-        """(zs, layer_start, layer_prims, rects) of the current primitives."""
-        prims = []
-        index = {}
-        start = [0]
-        flat = []
+        """Layer and primitive tables of FDTD_structured_values for the current
+        primitive parameters: (zs, layer_start, layer_prims, prim_info,
+        prim_vals, parts, verts)."""
+        prims, index, start, flat = [], {}, [0], []
         for layer in self._layers:
             for p in layer:
                 if id(p) not in index:
@@ -215,12 +320,31 @@ class StructuredMaterial3D(Material3D):
                     prims.append(p)
                 flat.append(index[id(p)])
             start.append(len(flat))
-        rects = np.zeros((max(len(prims), 1), 6))
-        for q, p in enumerate(prims):
+        info, vals, parts, verts = [], [], [], []
+        for p in prims:
+            if isinstance(p, Rectangle):
+                x0, x1, y0, y1 = p.bounds()
+                outline = np.array([[x0, y0], [x1, y0], [x1, y1], [x0, y1]])
+                pieces = [outline]
+            else:
+                outline = p.outline()
+                pieces = _convex_parts(outline)
+            ov = len(verts)
+            verts.extend(outline.tolist())
+            pp = len(parts)
+            for piece in pieces:
+                parts.append((len(verts), len(piece)))
+                verts.extend(np.asarray(piece).tolist())
+            info.append((ov, len(outline), pp, len(pieces)))
             m = complex(p.material_value)
-            rects[q] = (*p.bounds(), m.real, m.imag)
+            vals.append((m.real, m.imag, outline[:, 0].min(), outline[:, 0].max(),
+                         outline[:, 1].min(), outline[:, 1].max()))
+        i32 = lambda a, w: np.asarray(a if len(a) else [[0] * w], dtype=np.int32).reshape(-1)
         return (np.asarray(self._zs, dtype=np.float64), np.asarray(start, dtype=np.int32),
-                np.asarray(flat if flat else [0], dtype=np.int32), rects, len(prims))
+                np.asarray(flat if flat else [0], dtype=np.int32), i32(info, 4),
+                np.asarray(vals if vals else [[0.0] * 6], dtype=np.float64).reshape(-1),
+                i32(parts, 2), np.asarray(verts if verts else [[0.0, 0.0]], dtype=np.float64).reshape(-1),
+                len(prims), len(parts), len(verts))
 
     def get_values(self, k1, k2, j1, j2, i1, i2, sx=0, sy=0, sz=0, arr=None, reshape=True,
                    device=None):
@@ -228,7 +352,7 @@ class StructuredMaterial3D(Material3D):
         k1 <= k < k2, j1 <= j < j2, i1 <= i < i2, shaped [i, j, k].  With
         ``device`` (a CUDA device index or torch device) the result is a torch
         tensor on that GPU; otherwise a numpy array (``arr`` if given)."""
-        zs, start, flat, rects, nrects = self.tables()
+        zs, start, flat, info, vals, parts, verts, nprims, nparts, nverts = self.tables()
         shape = (i2 - i1, j2 - j1, k2 - k1)
         if device is not None:
             import torch
@@ -245,7 +369,8 @@ class StructuredMaterial3D(Material3D):
         if np.prod(shape) > 0:
             rc = libFDTD.FDTD_structured_values(
                 dev_index, stream, zs.ctypes.data if len(zs) else None, len(zs), start.ctypes.data,
-                flat.ctypes.data, rects.ctypes.data, nrects, self._dx, self._dy, self._dz,
+                flat.ctypes.data, info.ctypes.data, vals.ctypes.data, nprims, parts.ctypes.data,
+                nparts, verts.ctypes.data, nverts, self._dx, self._dy, self._dz,
                 k1, k2, j1, j2, i1, i2, float(sx), float(sy), float(sz), ptr, msg, 256)
             if rc != _ct.FDTD_OK:
                 raise _ct.FDTDError(msg.value.decode())

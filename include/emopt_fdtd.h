@@ -308,20 +308,24 @@ int FDTD_slab_finish(FDTDHandle *h, long long n0, long long Tn);
 int FDTD_amp_phase_noalloc(int device, void *stream, fdtd_complex128 *a, long long n, char *msg,
                            int msglen);
 
-/* ---- layered rectangle materials on the GPU (replaces the host evaluation
- * of the reference's StructuredMaterial3D with Rectangle primitives,
- * src/Grid.cpp:203-300 and :460-874, bound by emopt/grid_ctypes.py).
+/* ---- layered materials on the GPU (replaces the host evaluation of the
+ * reference's StructuredMaterial3D with Rectangle and Polygon primitives,
+ * src/Grid.cpp:203-395 and :460-874, bound by emopt/grid_ctypes.py).
  * zs[0..nzs-1]: ascending layer boundaries; layer l (zs[l]..zs[l+1]) holds the
- * primitives layer_prims[layer_start[l] .. layer_start[l+1]) in priority order;
- * rects[6 p ..]: xmin, xmax, ymin, ymax, Re, Im of primitive p.  Writes the
- * values at fractional indices (k + sx, j + sy, i + sz) for k1 <= k < k2, ...
- * into out[(i - i1) (j2 - j1) (k2 - k1) + (j - j1) (k2 - k1) + (k - k1)]
- * (host or device memory), like StructuredMaterial3D::get_values. */
+ * primitives layer_prims[layer_start[l] .. layer_start[l+1]) in priority order.
+ * Primitive p: prim_info[4p..4p+3] = outline vertex start and count, convex
+ * part start and count; prim_vals[6p..6p+5] = Re, Im, xmin, xmax, ymin, ymax
+ * (outline bounding box).  Part q: parts[2q..2q+1] = vertex start and count
+ * (counter-clockwise, convex).  verts: x, y pairs of outlines and parts.
+ * Writes the values at fractional indices (k + sx, j + sy, i + sz),
+ * k1 <= k < k2, ..., into out[(i - i1)(j2 - j1)(k2 - k1) + (j - j1)(k2 - k1)
+ * + (k - k1)] (host or device memory), like StructuredMaterial3D::get_values. */
 int FDTD_structured_values(int device, void *stream, const double *zs, int nzs,
-                           const int *layer_start, const int *layer_prims, const double *rects,
-                           int nrects, double dx, double dy, double dz, int k1, int k2, int j1,
-                           int j2, int i1, int i2, double sx, double sy, double sz,
-                           fdtd_complex128 *out, char *msg, int msglen);
+                           const int *layer_start, const int *layer_prims, const int *prim_info,
+                           const double *prim_vals, int nprims, const int *parts, int nparts,
+                           const double *verts, int nverts, double dx, double dy, double dz,
+                           int k1, int k2, int j1, int j2, int i1, int i2, double sx, double sy,
+                           double sz, fdtd_complex128 *out, char *msg, int msglen);
 
 #ifdef __cplusplus
 }

@@ -1,11 +1,11 @@
-"""CPU tests of the layered rectangle materials: the oracle restatement on
-hand-computed cells, and the host-side layer tables of emopt_b200.grid
-against the oracle's layer stack."""
+"""CPU tests of the layered rectangle and polygon materials: the oracle
+restatement on hand-computed cells, the host-side triangulation, and the
+layer tables of emopt_b200.grid against the oracle's layer stack."""
 import numpy as np
 import pytest
 
 from emopt_b200 import grid as G
-from oracle.structured import LayerStack, layer_value
+from oracle.structured import LayerStack, _outline, _value, layer_value
 
 
 def test_layer_value_known_answers():
@@ -43,28 +43,86 @@ def test_z_averaging_known_answers():
     assert st.value(0, 0, 2.0, 1.0, 1.0, dz) == pytest.approx(0.5 * 9 + 0.0)
 
 
-def _random_layout(seed, n=10):
+def _random_polygon(rng):
+    """A simple, star-shaped (often concave) polygon: n angles with gaps below
+    pi around the centre, radii random."""
+    n = int(rng.integers(3, 9))
+    ang = (np.arange(n) + rng.uniform(0, 0.8, n)) * 2 * np.pi / n
+    rad = rng.uniform(0.2, 1.2, n)
+    cx, cy = rng.uniform(0, 4), rng.uniform(0, 3)
+    xs, ys = cx + rad * np.cos(ang), cy + rad * np.sin(ang)
+    if rng.uniform() < 0.5:                     # closed the emopt way, clockwise
+        xs, ys = np.append(xs[::-1], xs[-1]), np.append(ys[::-1], ys[-1])
+    return G.Polygon(xs, ys)
+
+
+def _oracle_prim(p):
+    m = complex(p.material_value)
+    if isinstance(p, G.Rectangle):
+        return (*p.bounds(), m)
+    return (p.outline().tolist(), m)
+
+
+def _random_layout(seed, n=10, polygons=False):
     rng = np.random.default_rng(seed)
     mat = G.StructuredMaterial3D(4.0, 3.0, 2.0, 0.1, 0.1, 0.1)
     st = LayerStack()
     for q in range(n):
-        r = G.Rectangle(rng.uniform(0, 4), rng.uniform(0, 3), rng.uniform(0.05, 2.5), rng.uniform(0.05, 2.0))
+        if polygons and rng.uniform() < 0.6:
+            r = _random_polygon(rng)
+        else:
+            r = G.Rectangle(rng.uniform(0, 4), rng.uniform(0, 3), rng.uniform(0.05, 2.5), rng.uniform(0.05, 2.0))
         r.material_value = complex(rng.uniform(1, 12), rng.uniform(0, 0.3))
         r.layer = int(rng.integers(0, 4))
         z1 = float(np.round(rng.uniform(0, 1.5), 2))
         z2 = z1 + float(np.round(rng.uniform(-0.1, 1.0), 2))
         mat.add_primitive(r, z1, z2)
-        st.add((*r.bounds(), complex(r.material_value)), r.layer, z1, z2)
+        st.add(_oracle_prim(r), r.layer, z1, z2)
     return mat, st
+
+
+def test_polygon_known_answers():
+    # a triangle holding the lower-right half of the cell [-0.5, 0.5]^2 (three
+    # corners on its edges are not inside, (0.5, -0.5) is): half the cell
+    tri = ([(-0.5 - 1e-9, -0.5 - 1e-9), (5.0, -0.5 - 1e-9), (5.0, 5.0)], 3.0)
+    assert layer_value([tri], 0.0, 0.0, 1.0, 1.0) == pytest.approx(0.5 * 3 + 0.5, rel=1e-6)
+    # an L-shaped (concave) polygon covering three quarters
+    L = ([(-2, -2), (2, -2), (2, 0), (0, 0), (0, 2), (-2, 2)], 5.0)
+    assert layer_value([L], 0.0, 0.0, 1.0, 1.0) == pytest.approx(0.75 * 5 + 0.25)
+    # a clockwise outline with a repeated closing vertex comes out
+    # counter-clockwise without the repeat
+    v = G.Polygon([0, 0, 2, 2, 0], [0, 2, 2, 0, 0]).outline()
+    assert len(v) == 4
+    assert np.sum(v[:, 0] * np.roll(v[:, 1], -1) - np.roll(v[:, 0], -1) * v[:, 1]) == pytest.approx(8.0)
+    # the triangulation of a concave outline covers it exactly
+
+    def tri_area(t):
+        return 0.5 * abs((t[1][0] - t[0][0]) * (t[2][1] - t[0][1]) - (t[1][1] - t[0][1]) * (t[2][0] - t[0][0]))
+
+    tris = G._convex_parts(G.Polygon([0, 2, 2, 1, 0], [0, 0, 2, 1, 2]).outline())
+    assert len(tris) == 3 and sum(tri_area(t) for t in tris) == pytest.approx(3.0)
 
 
 @pytest.mark.parametrize("seed", range(6))
 def test_layer_tables_match_oracle_stack(seed):
-    mat, st = _random_layout(seed)
-    zs, start, flat, rects, nrects = mat.tables()
+    mat, st = _random_layout(seed, polygons=True)
+    zs, start, flat, info, vals, parts, verts, nprims, nparts, nverts = mat.tables()
     assert list(zs) == st.zs
     assert len(start) == len(st.layers) + 1
+    verts = verts.reshape(-1, 2)
+    info = info.reshape(-1, 4)
+    vals = vals.reshape(-1, 6)
     for l, layer in enumerate(st.layers):
-        got = [tuple(rects[flat[q]][:4]) + (complex(rects[flat[q]][4], rects[flat[q]][5]),)
-               for q in range(start[l], start[l + 1])]
-        assert got == [tuple(p) for p, _ in layer]
+        got = []
+        for q in range(start[l], start[l + 1]):
+            pr = flat[q]
+            ov, on = info[pr][0], info[pr][1]
+            got.append((verts[ov:ov + on].tolist(), complex(vals[pr][0], vals[pr][1])))
+        want = [(_outline(p), _value(p)) for p, _ in layer]
+        assert [(np.asarray(a).tolist(), b) for a, b in got] == [(np.asarray(a).tolist(), b) for a, b in want]
+
+
+def test_self_crossing_polygon_is_rejected():
+    bowtie = G.Polygon([0, 1, 1, 0], [0, 1, 0, 1])
+    with pytest.raises(ValueError, match="cross"):
+        G._convex_parts(bowtie.outline())
