@@ -261,8 +261,8 @@ class AdjointSolver:
     design written into device material arrays and the phasors kept on the
     device.  ``monitor`` is the raw-field box the figure of merit reads."""
 
-    def __init__(self, sim, design: PlanarDesign, monitor: DomainCoordinates,
-                 base_mats, device: int = 0, discrete_time: bool = False):
+    def __init__(self, sim, design: PlanarDesign, monitor, base_mats, device: int = 0,
+                 discrete_time: bool = False):
         self.sim = sim
         # The reference's A = diag(1j eps, ...) takes the CW frequency as 1 (in
         # units of omega).  The leapfrog's steady state obeys the same system
@@ -270,7 +270,10 @@ class AdjointSolver:
         # discrete solution carries that factor (1 - dt^2/24 + ...).
         self.dt_factor = float(np.sin(sim.dt / 2) / (sim.dt / 2)) if discrete_time else 1.0
         self.design = design
-        self.monitor = monitor
+        # one raw-field box or a list of them (e.g. a mode-match plane and the
+        # six planes of the source power)
+        self.monitors = list(monitor) if isinstance(monitor, (list, tuple)) else [monitor]
+        self.monitor = self.monitors[0]
         self.dev = torch.device("cuda", device)
         self.device = device
         shape = (sim.Nz, sim.Ny, sim.Nx)
@@ -282,9 +285,9 @@ class AdjointSolver:
         self._t1 = torch.zeros(shape, dtype=torch.complex128, device=self.dev)
         self.last = {}
 
-    # raw monitor block of the six components
-    def monitor_fields(self, which) -> torch.Tensor:
-        m = self.monitor
+    # raw block of the six components in monitor box m
+    def monitor_fields(self, which, m=None) -> torch.Tensor:
+        m = self.monitor if m is None else m
         return torch.stack([a[m.i1:m.i2, m.j1:m.j2, m.k1:m.k2] for a in which])
 
     def _set_eps(self, eps_cols: torch.Tensor):
@@ -329,25 +332,33 @@ class AdjointSolver:
         return {"steps": res.steps, "n_main": res.n_main, "device_ms": res.device_ms,
                 "total_ms": res.total_ms, "status": st}
 
-    def forward(self, eps_cols: torch.Tensor) -> torch.Tensor:
+    def forward(self, eps_cols: torch.Tensor):
         self._set_eps(eps_cols.detach())
         self.last["forward"] = self._solve(self.fwd, self.sim._sources, True)
-        return self.monitor_fields(self.fwd)
+        blocks = [self.monitor_fields(self.fwd, m) for m in self.monitors]
+        return blocks[0] if len(blocks) == 1 else tuple(blocks)
 
-    def backward(self, grad_monitor: torch.Tensor) -> torch.Tensor:
+    def backward(self, *grads) -> torch.Tensor:
+        """Adjoint solve with the currents dF/dx of every monitor box (boxes
+        that overlap add up, as the reference's adjoint source lists do,
+        emopt/adjoint_method.py:1458-1486), then the overlap kernel."""
         from .fdtd import SourceArray
-        m = self.monitor
-        dFdx = (torch.conj(grad_monitor) / 2).detach().cpu().numpy()
-        arrays = [np.ascontiguousarray(dFdx[c]).ravel() for c in range(6)]
-        I, J, K = m.i2 - m.i1, m.j2 - m.j1, m.k2 - m.k1
-        s = SourceArray(*arrays, m.i1, m.j1, m.k1, I, J, K)
-        # amplitude / phase conversion of the adjoint currents (src/fdtd.cpp:1517-1576)
         h = self.sim._libfdtd
         _ct.libFDTD.FDTD_clear_sources(h)
-        _ct.libFDTD.FDTD_add_source(h, s.Jx, s.Jy, s.Jz, s.Mx, s.My, s.Mz,
-                                    s.i0, s.j0, s.k0, s.I, s.J, s.K, True)
-        _ct.check(h, "FDTD_add_source")
-        self.last["adjoint"] = self._solve(self.adj, [s], False)
+        srcs = []
+        for m, g in zip(self.monitors, grads):
+            if g is None:
+                continue
+            dFdx = (torch.conj(g) / 2).detach().cpu().numpy()
+            arrays = [np.ascontiguousarray(dFdx[c]).ravel() for c in range(6)]
+            I, J, K = m.i2 - m.i1, m.j2 - m.j1, m.k2 - m.k1
+            s = SourceArray(*arrays, m.i1, m.j1, m.k1, I, J, K)
+            # amplitude / phase conversion of the adjoint currents (src/fdtd.cpp:1517-1576)
+            _ct.libFDTD.FDTD_add_source(h, s.Jx, s.Jy, s.Jz, s.Mx, s.My, s.Mz,
+                                        s.i0, s.j0, s.k0, s.I, s.J, s.K, True)
+            _ct.check(h, "FDTD_add_source")
+            srcs.append(s)
+        self.last["adjoint"] = self._solve(self.adj, srcs, False)
         return self.grad_eps()
 
     def grad_eps(self) -> torch.Tensor:
@@ -368,7 +379,8 @@ class AdjointSolver:
 
 
 class CWSolve(torch.autograd.Function):
-    """eps columns (3, nj, nk) -> raw monitor fields (6, mz, my, mx), complex128."""
+    """eps columns (3, nj, nk) -> raw fields (6, mz, my, mx), complex128, of
+    each monitor box (a tuple when the solver has several)."""
 
     @staticmethod
     def forward(ctx, eps_cols, solver: AdjointSolver):
@@ -376,8 +388,55 @@ class CWSolve(torch.autograd.Function):
         return solver.forward(eps_cols)
 
     @staticmethod
-    def backward(ctx, grad_out):
-        return ctx.solver.backward(grad_out), None
+    def backward(ctx, *grads):
+        return ctx.solver.backward(*grads), None
+
+
+def source_power_planes(sim):
+    """The six planes one cell inside the CPML through which the source power
+    is measured (emopt/fdtd.py:1555-1667), as (domain, normal axis, sign) with
+    the planes on symmetric min faces ('E' / 'H') left out."""
+    dx, dy, dz = sim.dx, sim.dy, sim.dz
+    w = sim._w_pml
+    X, Y, Z = sim.X, sim.Y, sim.Z
+    xmin = w[0] + dx if w[0] > 0 else 0.0
+    xmax = X - w[1] - dx if w[1] > 0 else X - dx
+    ymin = w[2] + dy if w[2] > 0 else 0.0
+    ymax = Y - w[3] - dy if w[3] > 0 else Y - dy
+    zmin = w[4] + dz if w[4] > 0 else 0.0
+    zmax = Z - w[5] - dz if w[5] > 0 else Z - dz
+    D = lambda a, b, c, d, e, f: DomainCoordinates(a, b, c, d, e, f, dx, dy, dz)
+    bc = sim.bc
+    planes = []
+    if bc[0] not in "EH":
+        planes.append((D(xmin, xmin, ymin, ymax, zmin, zmax), 0, -1.0))
+    planes.append((D(xmax, xmax, ymin, ymax, zmin, zmax), 0, 1.0))
+    if bc[1] not in "EH":
+        planes.append((D(xmin, xmax, ymin, ymin, zmin, zmax), 1, -1.0))
+    planes.append((D(xmin, xmax, ymax, ymax, zmin, zmax), 1, 1.0))
+    if bc[2] not in "EH":
+        planes.append((D(xmin, xmax, ymin, ymax, zmin, zmin), 2, -1.0))
+    planes.append((D(xmin, xmax, ymin, ymax, zmax, zmax), 2, 1.0))
+    return planes
+
+
+def source_power(raws, planes, grown, sim) -> torch.Tensor:
+    """Torch form of ``FDTD.get_source_power`` (emopt/fdtd.py:1555-1667):
+    0.5 * dA * sum Re(E x H*) . n over the six planes, from the raw blocks
+    ``raws`` of the grown plane domains ``grown``."""
+    dA = {0: sim.dy * sim.dz, 1: sim.dx * sim.dz, 2: sim.dx * sim.dy}
+    P = torch.zeros((), dtype=torch.float64, device=raws[0].device)
+    for raw, (dom, axis, sign), g in zip(raws, planes, grown):
+        f = {c: interp_field(raw[q], c, dom, g, sim.bc) for q, c in enumerate(COMPONENTS)}
+        cj = torch.conj
+        if axis == 0:
+            s = f["Ey"] * cj(f["Hz"]) - f["Ez"] * cj(f["Hy"])
+        elif axis == 1:
+            s = -(f["Ex"] * cj(f["Hz"]) - f["Ez"] * cj(f["Hx"]))
+        else:
+            s = f["Ex"] * cj(f["Hy"]) - f["Ey"] * cj(f["Hx"])
+        P = P + sign * 0.5 * dA[axis] * torch.sum(s.real)
+    return P
 
 
 class ModeMatchObjective(torch.nn.Module):
@@ -416,12 +475,41 @@ class ModeMatchObjective(torch.nn.Module):
         return self.mm(f)
 
 
+class PowerNormModeMatchObjective(ModeMatchObjective):
+    """The mode match divided by the source power, F = f / Psrc -- the
+    reference's power-normalized figure of merit (emopt/adjoint_method.py:
+    1418-1486 with fomutils.power_norm_dFdx_3D): the solver's monitors are the
+    mode-match box followed by the six grown source-power planes of
+    :func:`source_power_planes`, and autograd gives the adjoint currents on all
+    seven boxes."""
+
+    def __init__(self, solver: AdjointSolver, plane: DomainCoordinates, mode: dict, normal, **kw):
+        super().__init__(solver, plane, mode, normal, **kw)
+        sim = solver.sim
+        self.planes = source_power_planes(sim)
+        self.grown = solver.monitors[1:]
+        if len(self.grown) != len(self.planes):
+            raise ValueError("the solver needs the mode-match box and the source-power planes as monitors")
+
+    def forward(self, rho: torch.Tensor) -> torch.Tensor:
+        eps = self.solver.design.eps_columns(self.density(rho))
+        raws = CWSolve.apply(eps, self.solver)
+        f = {}
+        for c in self.components:
+            q = COMPONENTS.index(c)
+            f[c] = interp_field(raws[0][q], c, self.plane, self.interp_domain, self.bc).reshape(
+                self.mm.m[c].shape)
+        self.last_power = source_power(raws[1:], self.planes, self.grown, self.solver.sim)
+        return self.mm(f) / self.last_power
+
+
 def mmi_objective(p, precision: str = "fp64", kernel: str = "auto", device: int = 0,
-                  discrete_time: bool = False):
+                  discrete_time: bool = False, power_norm: bool = False):
     """The mode-match objective of :func:`emopt_b200.problems.mmi_gradient`:
     returns (objective module, design parameters as a float64 CUDA tensor).
     ``discrete_time``: include the leapfrog's frequency factor in the gradient
-    (exact for the time-stepped solution; the reference omits it)."""
+    (exact for the time-stepped solution; the reference omits it).
+    ``power_norm``: divide by the source power (the reference's PNF3D form)."""
     from .problems import EPS_SI, EPS_SIO2, make_solver
     sim = make_solver(p, precision=precision, kernel=kernel, device=device)
     dev = torch.device("cuda", device)
@@ -431,7 +519,12 @@ def mmi_objective(p, precision: str = "fp64", kernel: str = "auto", device: int 
     d = (p.dx, p.dy, p.dz)
     plane = DomainCoordinates.from_indices(k, k + 1, j1, j2, i1, i2, *d)
     monitor = grow_domain(plane, p.shape, d)
-    solver = AdjointSolver(sim, design, monitor, p.mats, device, discrete_time)
-    obj = ModeMatchObjective(solver, plane, p.fom_mode, (1, 0, 0))
+    if power_norm:
+        monitors = [monitor] + [grow_domain(dom, p.shape, d) for dom, _, _ in source_power_planes(sim)]
+        solver = AdjointSolver(sim, design, monitors, p.mats, device, discrete_time)
+        obj = PowerNormModeMatchObjective(solver, plane, p.fom_mode, (1, 0, 0))
+    else:
+        solver = AdjointSolver(sim, design, monitor, p.mats, device, discrete_time)
+        obj = ModeMatchObjective(solver, plane, p.fom_mode, (1, 0, 0))
     params = torch.as_tensor(p.design_params, dtype=torch.float64, device=dev)
     return obj, params

@@ -754,6 +754,26 @@ int FDTD_set_kernel(FDTDHandle* h, int which) {
     return FDTD_OK;
 }
 
+int FDTD_host_register(void* ptr, long long bytes) {
+    if (!ptr || bytes <= 0) return FDTD_ERR_ARG;
+    cudaError_t e = cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();   // leave no error behind for later calls
+        return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? FDTD_ERR_NODEVICE : FDTD_ERR_CUDA;
+    }
+    return FDTD_OK;
+}
+
+int FDTD_host_unregister(void* ptr) {
+    if (!ptr) return FDTD_ERR_ARG;
+    cudaError_t e = cudaHostUnregister(ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return FDTD_ERR_CUDA;
+    }
+    return FDTD_OK;
+}
+
 }  // extern "C"
 
 // ================================================== device-resident solve

@@ -222,32 +222,21 @@ class FDTD(MaxwellSolver):
     PIN_LIMIT = 4 << 30
 
     def _pin(self, arrays):
-        total = sum(a.nbytes for a in arrays)
-        if total > self.PIN_LIMIT:
+        if sum(a.nbytes for a in arrays) > self.PIN_LIMIT:
             return
-        try:
-            import torch
-            cudart = torch._C._cudart
-        except (ImportError, AttributeError):
-            return
-        self._cudart = cudart          # kept for __del__, which may run at shutdown
         for a in arrays:
-            ptr = a.ctypes.data
-            if int(cudart.cudaHostRegister(ptr, a.nbytes, 1)) == 0:   # cudaHostRegisterPortable
-                self._pinned.append((ptr, a))
-            else:
+            if libFDTD.FDTD_host_register(a.ctypes.data, a.nbytes) != _ct.FDTD_OK:
                 break
+            self._pinned.append((a.ctypes.data, a))
 
     def __del__(self):
         h = getattr(self, "_libfdtd", None)
         if h:
             libFDTD.FDTD_delete(h)
             self._libfdtd = None
-        pinned = getattr(self, "_pinned", [])
-        if pinned:
-            for ptr, _ in pinned:
-                self._cudart.cudaHostUnregister(ptr)
-            self._pinned = []
+        for ptr, _ in getattr(self, "_pinned", []):
+            libFDTD.FDTD_host_unregister(ptr)
+        self._pinned = []
 
     # ------------------------------------------------------------ properties
     @property

@@ -184,6 +184,11 @@ libFDTD.FDTD_slab_capture.restype = c_int
 libFDTD.FDTD_slab_finish.argtypes = [c_void_p, c_longlong, c_longlong]
 libFDTD.FDTD_slab_finish.restype = c_int
 
+libFDTD.FDTD_host_register.argtypes = [c_void_p, c_longlong]
+libFDTD.FDTD_host_register.restype = c_int
+libFDTD.FDTD_host_unregister.argtypes = [c_void_p]
+libFDTD.FDTD_host_unregister.restype = c_int
+
 # layered materials (emopt_b200/grid.py)
 libFDTD.FDTD_structured_values.argtypes = [c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
                                            c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p,
@@ -199,7 +204,8 @@ ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_
                  "FDTD_serve_finished", "FDTD_serve_collect", "FDTD_serve_info",
                  "FDTD_serve_delete", "FDTD_set_stream", "FDTD_slab_set", "FDTD_slab_begin",
                  "FDTD_slab_step", "FDTD_slab_halo", "FDTD_slab_sample", "FDTD_slab_probe",
-                 "FDTD_slab_capture", "FDTD_slab_finish", "FDTD_structured_values")
+                 "FDTD_slab_capture", "FDTD_slab_finish", "FDTD_structured_values",
+                 "FDTD_host_register", "FDTD_host_unregister")
 
 
 class FDTDError(RuntimeError):

@@ -132,6 +132,14 @@ int FDTD_set_precision(FDTDHandle *h, int bits);
  * Periodic boundaries always use 1. */
 int FDTD_set_kernel(FDTDHandle *h, int which);
 
+/* Page-locks (cudaHostRegister, portable) / releases host memory that is
+ * copied to or from the GPU on every solve -- material and t0 arrays -- so
+ * those copies run at full DMA speed.  No counterpart in the reference.
+ * Returns FDTD_OK, FDTD_ERR_ARG, FDTD_ERR_NODEVICE or FDTD_ERR_CUDA and leaves
+ * no pending CUDA error behind. */
+int FDTD_host_register(void *ptr, long long bytes);
+int FDTD_host_unregister(void *ptr);
+
 typedef struct {
     long long Tn;              /* probe period and extraction spacing: int64(Ncycle*3/4) (emopt/fdtd.py:1021) */
     double Nmax;               /* step budget: the loop stops once n > Nmax (emopt/fdtd.py:1054) */

@@ -147,3 +147,40 @@ def test_calc_ydAx_topology_matches_reference_formula(planar):
     got = sim.calc_ydAx_topology(design, True, sig_e, sig_m, de, dm, planar, lam)
     assert got.shape == want.shape
     assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
+
+
+def test_source_power_matches_host_computation():
+    """The torch source power on the device phasors equals FDTD.get_source_power
+    (host numpy, emopt/fdtd.py:1555-1667) on the same fields."""
+    p = _problem(fixed_steps=600)
+    obj, params = A.mmi_objective(p, "fp64", power_norm=True)
+    with torch.no_grad():
+        obj(params)
+    sim = obj.solver.sim
+    for a, c in zip(obj.solver.fwd, ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")):
+        getattr(sim, "_%s_fwd_t0" % c)[:] = a.cpu().numpy().ravel()
+    P_host = sim.get_source_power()
+    assert obj.last_power.item() == pytest.approx(P_host, rel=1e-12)
+    assert P_host > 0
+
+
+def test_power_normalized_gradient_central_differences():
+    """F = mode match / source power (the reference's PNF3D form): adjoint
+    currents on the mode-match box and the six power planes, against central
+    differences on 8 seeded parameters."""
+    p = _problem(fixed_steps=N_FIXED)
+    obj, params = A.mmi_objective(p, "fp64", discrete_time=True, power_norm=True)
+    F0, g = _value_and_grad(obj, params)
+    idx = _indices(params.numel())[:8]
+    h = 1e-4
+    fd = np.empty(len(idx))
+    for n, q in enumerate(idx):
+        pp = params.clone()
+        pp.view(-1)[q] += h
+        pm = params.clone()
+        pm.view(-1)[q] -= h
+        with torch.no_grad():
+            fd[n] = (obj(pp).item() - obj(pm).item()) / (2 * h)
+    err = np.linalg.norm(fd - g[idx]) / np.linalg.norm(fd)
+    print("power-normalized: central FD vs adjoint %.3e" % err)
+    assert err < 2e-5
