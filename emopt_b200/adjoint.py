@@ -346,12 +346,16 @@ class AdjointSolver:
         h = self.sim._libfdtd
         _ct.libFDTD.FDTD_clear_sources(h)
         srcs = []
+        # the currents as complex boxes (before the library's amplitude/phase
+        # conversion), for solving the same adjoint problem elsewhere
+        self.last_adjoint_currents = []
         for m, g in zip(self.monitors, grads):
             if g is None:
                 continue
             dFdx = (torch.conj(g) / 2).detach().cpu().numpy()
             arrays = [np.ascontiguousarray(dFdx[c]).ravel() for c in range(6)]
             I, J, K = m.i2 - m.i1, m.j2 - m.j1, m.k2 - m.k1
+            self.last_adjoint_currents.append(([a.reshape(I, J, K).copy() for a in arrays], m.i1, m.j1, m.k1))
             s = SourceArray(*arrays, m.i1, m.j1, m.k1, I, J, K)
             # amplitude / phase conversion of the adjoint currents (src/fdtd.cpp:1517-1576)
             _ct.libFDTD.FDTD_add_source(h, s.Jx, s.Jy, s.Jz, s.Mx, s.My, s.Mz,

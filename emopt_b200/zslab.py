@@ -35,6 +35,10 @@ from . import fdtd_ctypes as _ct
 from .fdtd import derive_parameters
 from .fdtd_ctypes import libFDTD
 
+# the same library without argument types, for device pointers where the
+# typed binding expects host arrays
+_raw = ctypes.CDLL(_ct.so_path)
+
 
 def ownership(N: int, n: int) -> list[tuple[int, int]]:
     """(start, count) of the planes of each of ``n`` slabs: the first ``N % n``
@@ -105,7 +109,7 @@ class CudaSlab:
     """
 
     def __init__(self, p, i0: int, I: int, precision: str = "fp32", device: int = 0,
-                 stream: int | None = None):
+                 stream: int | None = None, t0_device: bool = False):
         prm = derive_parameters(p.X, p.Y, p.Z, p.dx, p.dy, p.dz, p.wavelength, 1.0,
                                 p.nconv or 10)
         Nx, Ny, Nz = prm["Nx"], prm["Ny"], prm["Nz"]
@@ -137,9 +141,17 @@ class CudaSlab:
         libFDTD.FDTD_set_source_properties(h, src_T, prm["src_min"])
         libFDTD.FDTD_set_bc(h, p.bc.encode("ascii"))
         n = Nx * Ny * I
-        self.t0 = [np.zeros(n, dtype=np.complex128) for _ in range(6)]
         self._t1 = [np.zeros(n, dtype=np.complex128) for _ in range(6)]
-        libFDTD.FDTD_set_t0_arrays(h, *self.t0)
+        self.t0_device = t0_device
+        if t0_device:
+            # phasors stay on the GPU (torch tensors the extraction writes into)
+            import torch
+            self.t0 = [torch.zeros((I, Ny, Nx), dtype=torch.complex128,
+                                   device=torch.device("cuda", device)) for _ in range(6)]
+            _raw.FDTD_set_t0_arrays(h, *[ctypes.c_void_p(t.data_ptr()) for t in self.t0])
+        else:
+            self.t0 = [np.zeros(n, dtype=np.complex128) for _ in range(6)]
+            libFDTD.FDTD_set_t0_arrays(h, *self.t0)
         libFDTD.FDTD_set_t1_arrays(h, *self._t1)
         # sources cropped to the slab, in slab coordinates, converted to
         # amplitude/phase by the library (emopt/fdtd.py:710-747)
@@ -202,6 +214,8 @@ class CudaSlab:
 
     def finish(self, n0: int, Tn: int):
         self._ok(libFDTD.FDTD_slab_finish(self.h, n0, Tn), "FDTD_slab_finish")
+        if self.t0_device:
+            return list(self.t0)
         return [a.reshape(self.I, self.Ny, self.Nx) for a in self.t0]
 
     def close(self):
@@ -348,7 +362,7 @@ class SlabSet:
     """
 
     def __init__(self, p, ranges, precision="fp32", devices=None, link=None, rank=None,
-                 stream=None):
+                 stream=None, t0_device=False):
         prm = derive_parameters(p.X, p.Y, p.Z, p.dx, p.dy, p.dz, p.wavelength, 1.0, p.nconv or 10)
         Nx, Ny, Nz = prm["Nx"], prm["Ny"], prm["Nz"]
         self.p = p
@@ -370,7 +384,8 @@ class SlabSet:
         self.slabs = []
         try:
             for s, d, st in zip(self.mine, devs, streams):
-                self.slabs.append(CudaSlab(p, *ranges[s], precision=precision, device=d, stream=st))
+                self.slabs.append(CudaSlab(p, *ranges[s], precision=precision, device=d, stream=st,
+                                           t0_device=t0_device))
         except Exception:
             self.close()
             raise
@@ -395,6 +410,45 @@ class SlabSet:
     def close(self):
         for s in self.slabs:
             s.close()
+
+
+def grad_eps_planar(fwd, adj, box, ranges, link, device=0):
+    """Permittivity gradient of a planar design over the slabs: each slab runs
+    the fused overlap ``FDTD_grad_eps`` (Kahan z-sums) on its own planes of the
+    design layer, and the per-column partial sums are added over the slabs --
+    in one process directly, over ranks with an all-reduce (``link``).
+
+    ``fwd`` / ``adj``: {slab index: six device phasor tensors [I, Ny, Nx]} of
+    the slabs this process holds (``SlabSet(..., t0_device=True).finish()``);
+    ``box``: k0, k1, j0, j1 and the z range [i0_c, i1_c) of each E component
+    in global planes.  Returns the (3, j1 - j0, k1 - k0) float64 tensor that
+    ``adjoint.AdjointSolver.grad_eps`` gives on one GPU."""
+    import torch
+    k0, k1, j0, j1 = box[:4]
+    dev = torch.device("cuda", device)
+    total = torch.zeros((3, j1 - j0, k1 - k0), dtype=torch.float64, device=dev)
+    for s, F in fwd.items():
+        i0s, I = ranges[s]
+        A = adj[s]
+        Iz, Ny, Nx = F[0].shape
+        local = [k0, k1, j0, j1]
+        for c in range(3):
+            a, b = box[4 + 2 * c], box[5 + 2 * c]
+            lo, hi = max(a, i0s), min(b, i0s + I)
+            local += [lo - i0s, hi - i0s] if lo < hi else [0, 0]
+        out = torch.empty((3, j1 - j0, k1 - k0), dtype=torch.float64, device=F[0].device)
+        fp = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in F[:3]])
+        ap = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in A[:3]])
+        msg = ctypes.create_string_buffer(256)
+        st = libFDTD.FDTD_grad_eps(F[0].device.index, torch.cuda.current_stream(F[0].device).cuda_stream,
+                                   fp, ap, Nx, Ny, Iz, (ctypes.c_int * 10)(*local), 1,
+                                   ctypes.c_void_p(out.data_ptr()), msg, len(msg))
+        if st != _ct.FDTD_OK:
+            raise _ct.FDTDError(msg.value.decode())
+        total += out.to(dev)
+    if isinstance(link, TorchLink):
+        link.dist.all_reduce(total)
+    return total
 
 
 def solve(p, ranges, precision="fp32", devices=None, link=None, rank=None, stream=None):
