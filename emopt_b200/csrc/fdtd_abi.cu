@@ -23,6 +23,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/emopt_fdtd.h"
 #include "kernels.h"
 
@@ -1048,8 +1050,31 @@ long long probe_offset(const FDTDHandle* h, int px, long long pidx) {
     return ((c[2] - 1) * h->Ny + (c[1] - 1)) * (long long)px + (c[0] - 1);
 }
 
+// Named ranges on the profiler timeline (NVTX; free when no tool listens).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+
+// Consecutive phases: next() closes the open range and opens another; the
+// last one closes on scope exit, early returns included.
+struct NvtxPhases {
+    bool open = false;
+    void next(const char* name) {
+        if (open) nvtxRangePop();
+        nvtxRangePushA(name);
+        open = true;
+    }
+    ~NvtxPhases() {
+        if (open) nvtxRangePop();
+    }
+};
+
 template <typename T>
 int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
+    NvtxRange call("FDTD_solve_cw");
+    NvtxPhases phase;
+    phase.next("set-up: materials, sources, step table");
     if (!h->whole_grid())
         return h->fail(FDTD_ERR_ARG, "FDTD_solve_cw needs the whole grid as the local chunk");
     if (h->slab) return h->fail(FDTD_ERR_ARG, "the handle is a z slab: it is stepped by FDTD_slab_*");
@@ -1191,6 +1216,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     };
 
     CK(cudaEventRecord(h->ev[0], h->stream));
+    phase.next("time loop with convergence probes");
     long long n = 0;
     double Ach = 1, Pch = 1;
     double amp_rtol = o->rtol, phi_rtol = sqrt(o->rtol);
@@ -1219,6 +1245,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
             CK(cudaStreamSynchronize(h->stream));
             Ach = h->pinned[0];
             Pch = h->pinned[1];
+            if (o->stop_nonfinite && !(std::isfinite(Ach) && std::isfinite(Pch))) break;
         }
     }
     if (fixed) {
@@ -1227,6 +1254,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
         Ach = h->pinned[0];
         Pch = h->pinned[1];
     }
+    phase.next("t0/t1 captures and 2 Tn steps");
     const long long n0 = n;
     for (int c = 0; c < 6; c++)
         CK(cudaMemcpyAsync(r.snap[0][c].p, cur_set(n0)[c], sizeof(T) * cells, cudaMemcpyDeviceToDevice, h->stream));
@@ -1235,6 +1263,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
         CK(cudaMemcpyAsync(r.snap[1][c].p, cur_set(n0 + Tn)[c], sizeof(T) * cells, cudaMemcpyDeviceToDevice, h->stream));
     if ((rc = run(n0 + Tn, Tn)) != FDTD_OK) return rc;
     CK(cudaEventRecord(h->ev[1], h->stream));
+    phase.next("3-sample extraction and copy-out");
 
     // 3-sample extraction (src/fdtd.cpp:1346-1443) with t0 = n0 dt,
     // t1 = (n0+Tn) dt, t2 = (n0+2Tn) dt; H samples half a step earlier.

@@ -153,7 +153,8 @@ struct ServeCtl {
     long long Tn, last, n0, nprobes;
     double Nmax, amp_tol, phi_tol, dt, A_change, phi_change;
     ProbeDev pd;
-    int state, capture, fixed, pad;
+    int state, capture, fixed;
+    int stop_nf;            // 1: a probe that sees NaN/Inf ends the main loop
 };
 
 template <typename T>

@@ -262,6 +262,7 @@ extern "C" int FDTD_serve_admit(FDTDServe* s, FDTDHandle* h, const FDTDSolveOpti
     c.phi_tol = sqrt(o->rtol);
     c.dt = h->dt;
     c.fixed = fixed ? 1 : 0;
+    c.stop_nf = o->stop_nonfinite ? 1 : 0;
     c.pd.win = dptr<double>(r.pwin); c.pd.A = dptr<double>(r.pA); c.pd.phi = dptr<double>(r.pphi);
     c.pd.times = dptr<double>(r.ptimes); c.pd.out = dptr<double>(r.pout); c.pd.map = dptr<long long>(r.pmap);
     c.pd.nconv = nconv;
@@ -286,6 +287,7 @@ extern "C" int FDTD_serve_admit(FDTDServe* s, FDTDHandle* h, const FDTDSolveOpti
 // collected, or -(status) on an error.
 extern "C" int FDTD_serve_advance(FDTDServe* s) {
     if (!s) return -FDTD_ERR_ARG;
+    NvtxRange range("FDTD_serve_advance");
     if (!s->exec) return -s->fail(FDTD_ERR_CUDA, "engine not initialised");
     SCK(cudaSetDevice(s->device));
     SCK(cudaGraphLaunch(s->exec, s->stream));

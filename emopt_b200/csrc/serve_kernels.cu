@@ -120,7 +120,8 @@ __global__ void __launch_bounds__(256) k_serve_events(const ServeView<T>* __rest
             const bool finite = !(isnan(A) || isinf(A) || isnan(P) || isinf(P));
             const bool converged = !c.fixed && finite && !(A > c.amp_tol) && !(P > c.phi_tol);
             int next = SERVE_RUN;
-            if (converged || (double)n > (c.fixed ? (double)c.last : c.Nmax)) next = SERVE_EXTRACT;
+            if (converged || (c.stop_nf && !finite) || (double)n > (c.fixed ? (double)c.last : c.Nmax))
+                next = SERVE_EXTRACT;
             else if (n + c.Tn - 1 > c.last) next = SERVE_TAIL;
             if (next == SERVE_EXTRACT) { c.n0 = n; c.capture = 1; atomicAdd(cap_count, 1); }
             else c.capture = 0;

@@ -217,6 +217,9 @@ class FDTD(MaxwellSolver):
         self.adjoint_count = 0
         self.last_solve = None
         self.fixed_steps = None
+        # True: a solve whose convergence probe sees NaN/Inf stops there (status
+        # NONFINITE) instead of running on to Nmax as the reference does
+        self.stop_nonfinite = False
 
     # at most this many bytes of one solver's host arrays are page-locked
     PIN_LIMIT = 4 << 30
@@ -496,6 +499,7 @@ class FDTD(MaxwellSolver):
         opt.fixed_steps = int(self.fixed_steps) if self.fixed_steps else 0
         opt.materials_unchanged = 0 if self._materials_dirty else 1
         opt.copy_t1 = 0
+        opt.stop_nonfinite = 1 if self.stop_nonfinite else 0
         res = _ct.SolveResult()
         status = libFDTD.FDTD_solve_cw(h, ctypes.byref(opt), ctypes.byref(res))
         if status not in (_ct.FDTD_OK, _ct.FDTD_NMAX, _ct.FDTD_NONFINITE):

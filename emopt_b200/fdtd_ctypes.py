@@ -112,7 +112,7 @@ class SolveOptions(Structure):
     _fields_ = [("Tn", c_longlong), ("Nmax", c_double), ("rtol", c_double),
                 ("conv_pts", POINTER(c_longlong)), ("nconv", c_int),
                 ("fixed_steps", c_longlong), ("materials_unchanged", c_int),
-                ("copy_t1", c_int)]
+                ("copy_t1", c_int), ("stop_nonfinite", c_int)]
 
 
 class SolveResult(Structure):

@@ -149,6 +149,8 @@ typedef struct {
     long long fixed_steps;     /* > 0: run exactly this many main steps without a convergence test */
     int materials_unchanged;   /* 1: reuse the coefficients of the previous solve on this handle */
     int copy_t1;               /* 1: also write the t1 snapshot into .real of the t1 arrays */
+    int stop_nonfinite;        /* 1: end the main loop at the first probe that sees NaN/Inf
+                                  (status FDTD_NONFINITE); 0: run on to Nmax as the reference */
 } FDTDSolveOptions;
 
 typedef struct {

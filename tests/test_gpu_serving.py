@@ -123,3 +123,34 @@ def test_budget_admission_waits_for_memory(mu_ones):
     assert len(done) == 2
     assert done[0][0]["steps"] == done[1][0]["steps"]
     assert _rel(done[1][1], done[0][1]) < 1e-6
+
+
+def test_nonfinite_request_retires_early(alone_solve_cw, mu_ones):
+    """A request whose permittivity holds NaN and that asks to stop on a
+    non-finite probe retires at its first probe with status NONFINITE; a
+    request served beside it gives its solo result."""
+    specs = _specs()
+    bad = S.Request(specs[0], 0, mu_ones)
+    for e in bad.eps:
+        e.view(-1)[: e.numel() // 2] = float("nan")
+    bad.opt.stop_nonfinite = 1
+    good = S.Request(specs[1], 0, mu_ones)
+    torch.cuda.synchronize()
+    eng = S.ServeEngine(0, 8e9, 4, 16)
+    res = {}
+    try:
+        assert eng.admit(bad) and eng.admit(good)
+        while eng.active:
+            for req, r in eng.collect(eng.advance()):
+                res[req.spec.rid] = (r, [a.cpu().numpy() for a in req.out])
+                req.close()
+    finally:
+        eng.close()
+    r_bad, _ = res[specs[0].rid]
+    Tn = bad.opt.Tn
+    assert r_bad["status"] == ct.FDTD_NONFINITE
+    assert r_bad["nprobes"] == 1 and r_bad["steps"] == 3 * Tn
+    r_good, F = res[specs[1].rid]
+    steps, n_main, F1 = alone_solve_cw[specs[1].rid]
+    assert r_good["status"] == ct.FDTD_OK and r_good["steps"] == steps
+    assert _rel(F, F1) < 1e-6
