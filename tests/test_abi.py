@@ -37,7 +37,7 @@ def test_reference_binding_loads_unchanged():
 
 def test_struct_layouts():
     from emopt_b200 import fdtd_ctypes as ct
-    assert ctypes.sizeof(ct.SolveOptions) == 56
+    assert ctypes.sizeof(ct.SolveOptions) == 64
     assert ctypes.sizeof(ct.SolveResult) == 72
 
 
