@@ -1026,6 +1026,10 @@ fdtdb::GridView<T> make_view(FDTDHandle* h, Resident<T>& r, int set) {
         P.bE = dptr<T>(r.tab[a][4]); P.cE = dptr<T>(r.tab[a][5]);
     }
     g.zlo = g.zhi = 0;
+    g.chk = nullptr;
+#ifdef FDTD_BOUNDS_CHECK
+    g.chk = dptr<int>(r.err) + 1;
+#endif
     g.step_tab = dptr<double4>(r.steptab);
     return g;
 }
@@ -1109,7 +1113,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     CK(cudaEventRecord(h->ev[2], h->stream));
     if ((rc = alloc_resident<T>(h, r, fused)) != FDTD_OK) return rc;
     if (tma && !build_maps<T>(h, r)) tma = false;
-    CK(cudaMemsetAsync(r.err.p, 0, sizeof(int), h->stream));
+    CK(cudaMemsetAsync(r.err.p, 0, sizeof(int) * 4, h->stream));
     if (!o->materials_unchanged || !r.coeffs_valid) {
         if ((rc = prepare_materials<T>(h, r)) != FDTD_OK) return rc;
         launches += 3 + 3 + 3;   // eps coefficients, uniform checks, mu coefficients (upper bound)
@@ -1291,10 +1295,11 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
         }
     }
     CK(cudaEventRecord(h->ev[3], h->stream));
-    int kerr = 0;
-    CK(cudaMemcpyAsync(&kerr, r.err.p, sizeof(int), cudaMemcpyDefault, h->stream));
+    int kerr[2] = {0, 0};
+    CK(cudaMemcpyAsync(kerr, r.err.p, sizeof(int) * 2, cudaMemcpyDefault, h->stream));
     if ((rc = h->sync_check("FDTD_solve_cw")) != FDTD_OK) return rc;
-    if (kerr) return h->fail(FDTD_ERR_CUDA, "a bounded wait in the step kernel gave up (code %d)", kerr);
+    if (kerr[0]) return h->fail(FDTD_ERR_CUDA, "a bounded wait in the step kernel gave up (code %d)", kerr[0]);
+    if (kerr[1]) return h->fail(FDTD_ERR_CUDA, "bounds check: a step kernel computed an index outside its array (site %d)", kerr[1]);
     float ms_steps = 0, ms_total = 0;
     cudaEventElapsedTime(&ms_steps, h->ev[0], h->ev[1]);
     cudaEventElapsedTime(&ms_total, h->ev[2], h->ev[3]);

@@ -71,6 +71,7 @@ struct GridView {
     // Nz - 1 (zhi): the field arrays then have a halo plane there, filled by
     // the exchange, which is read instead of applying the boundary rule
     char zlo, zhi;
+    int* chk;                      // builds with FDTD_BOUNDS_CHECK: first failed index check (else unused)
     PmlAxis<T> pml[3];
     const double4* step_tab;       // per step: (S_H, C_H, S_E, C_E)
 };

@@ -235,7 +235,8 @@ extern "C" int FDTD_serve_admit(FDTDServe* s, FDTDHandle* h, const FDTDSolveOpti
           ck(cudaMemsetAsync(r.pA.p, 0, r.pA.bytes, h->stream), "probe") &&
           ck(cudaMemsetAsync(r.pphi.p, 0, r.pphi.bytes, h->stream), "probe") &&
           ck(cudaMemsetAsync(r.ptimes.p, 0, r.ptimes.bytes, h->stream), "probe") &&
-          ck(cudaMemsetAsync(r.pout.p, 0, r.pout.bytes, h->stream), "probe");
+          ck(cudaMemsetAsync(r.pout.p, 0, r.pout.bytes, h->stream), "probe") &&
+          ck(cudaMemsetAsync(r.err.p, 0, r.err.bytes, h->stream), "status");
     if (!okb) return hfail();
     std::vector<long long> map((size_t)nc, -1);
     for (int q = 0; q < nconv; q++) map[q] = probe_offset(h, r.px, o->conv_pts[q]);
@@ -335,7 +336,15 @@ extern "C" int FDTD_serve_collect(FDTDServe* s, FDTDHandle** done, FDTDSolveResu
             SCK(cudaGetLastError());
             SCK(cudaMemcpyAsync(h->ht0[comp], r.stage.p, sizeof(c128) * ncell, cudaMemcpyDefault, s->stream));
         }
+#ifdef FDTD_BOUNDS_CHECK
+        int kchk = 0;
+        SCK(cudaMemcpyAsync(&kchk, dptr<int>(r.err) + 1, sizeof(int), cudaMemcpyDefault, s->stream));
+#endif
         SCK(cudaStreamSynchronize(s->stream));
+#ifdef FDTD_BOUNDS_CHECK
+        if (kchk)
+            return -s->fail(FDTD_ERR_CUDA, "bounds check: the stepping kernel computed an index outside its array (site %d)", kchk);
+#endif
         FDTDSolveResult& o = res[k];
         std::memset(&o, 0, sizeof(o));
         o.n_main = n0;

@@ -53,7 +53,7 @@ int slab_begin_impl(FDTDHandle* h, const FDTDSolveOptions* o, const long long* c
     Resident<T>& r = resident<T>(h);
     int rc;
     if ((rc = alloc_resident<T>(h, r, false, 1)) != FDTD_OK) return rc;
-    CK(cudaMemsetAsync(r.err.p, 0, sizeof(int), h->stream));
+    CK(cudaMemsetAsync(r.err.p, 0, sizeof(int) * 4, h->stream));
     if (!o->materials_unchanged || !r.coeffs_valid)
         if ((rc = prepare_materials<T>(h, r)) != FDTD_OK) return rc;
     if ((rc = prepare_sources<T>(h, r, slab_src<T>(h))) != FDTD_OK) return rc;
@@ -195,11 +195,12 @@ int slab_finish_impl(FDTDHandle* h, long long n0, long long Tn) {
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(h->ht0[c], r.stage.p, sizeof(c128) * ncell, cudaMemcpyDefault, h->stream));
     }
-    int kerr = 0;
-    CK(cudaMemcpyAsync(&kerr, r.err.p, sizeof(int), cudaMemcpyDefault, h->stream));
+    int kerr[2] = {0, 0};
+    CK(cudaMemcpyAsync(kerr, r.err.p, sizeof(int) * 2, cudaMemcpyDefault, h->stream));
     int rc;
     if ((rc = h->sync_check("FDTD_slab_finish")) != FDTD_OK) return rc;
-    if (kerr) return h->fail(FDTD_ERR_CUDA, "a bounded wait in a step kernel gave up (code %d)", kerr);
+    if (kerr[0]) return h->fail(FDTD_ERR_CUDA, "a bounded wait in a step kernel gave up (code %d)", kerr[0]);
+    if (kerr[1]) return h->fail(FDTD_ERR_CUDA, "bounds check: a step kernel computed an index outside its array (site %d)", kerr[1]);
     return FDTD_OK;
 }
 

@@ -12,7 +12,10 @@
 // before any dependent instruction; the source test is made once per warp.
 // The source coefficients of the step are g.step_tab[*step_ctr + off].
 // Used by the single-solve kernels (vec_kernels.cu) and the batched serving
-// kernels (serve_kernels.cu).  Requires non-periodic boundaries.  In a z slab
+// kernels (serve_kernels.cu).  Requires non-periodic boundaries.  Built with
+// FDTD_BOUNDS_CHECK, every index a lane computes is checked against its
+// array first; a lane out of range records the site (GridView::chk) and
+// skips its accesses.  In a z slab
 // of a distributed solve (g.zlo / g.zhi) the neighbour plane across an inner
 // slab face is read from the halo plane of the field arrays, and the z CPML
 // index is taken at the global plane i + g.pml[2].off.
@@ -79,6 +82,42 @@ __device__ __forceinline__ bool sources_touch(const SourceList<T>& src, int comp
     return hit;
 }
 
+#ifdef FDTD_BOUNDS_CHECK
+// Debug builds: is idx in [lo, hi)?  The first failure records its site.
+template <typename T>
+__device__ bool in_range(const GridView<T>& g, long long idx, long long lo, long long hi, int site) {
+    if (idx >= lo && idx < hi) return true;
+    if (g.chk) atomicCAS(g.chk, 0, site);
+    return false;
+}
+
+// Every field vector (and scalar) the H body of this lane reads and writes.
+template <typename T>
+__device__ bool h_fields_ok(const GridView<T>& g, int i, int j, int k0, int lane, long long p) {
+    constexpr int V = V16<T>::N;
+    const long long plane = g.plane, top = (long long)g.Nz * plane;
+    const long long fhi = ((long long)g.Nz + (g.zhi ? 1 : 0)) * plane;
+    bool ok = in_range(g, p, 0, top - V + 1, 1);
+    if (j + 1 < g.Ny) ok &= in_range(g, p + g.px, 0, top - V + 1, 2);
+    if (i + 1 < g.Nz || g.zhi) ok &= in_range(g, p + plane, 0, fhi - V + 1, 3);
+    if (lane == 31 && k0 + V < g.Nx) ok &= in_range(g, p + V, 0, top, 4);
+    return ok;
+}
+
+// ... and the E body.
+template <typename T>
+__device__ bool e_fields_ok(const GridView<T>& g, int i, int j, int k0, int lane, long long p) {
+    constexpr int V = V16<T>::N;
+    const long long plane = g.plane, top = (long long)g.Nz * plane;
+    const long long flo = g.zlo ? -plane : 0;
+    bool ok = in_range(g, p, 0, top - V + 1, 11);
+    if (j > 0) ok &= in_range(g, p - g.px, 0, top - V + 1, 12);
+    if (i > 0 || g.zlo) ok &= in_range(g, p - plane, flo, top - V + 1, 13);
+    if (lane == 0 && k0 > 0) ok &= in_range(g, p - 1, 0, top, 14);
+    return ok;
+}
+#endif
+
 }  // namespace vecb
 
 template <typename T>
@@ -90,14 +129,25 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
     const int m = xb * 32 + lane;
     const int k0 = m * V;
     // Lanes beyond the row still take part in the shuffle below.
-    const bool act = j < g.Ny && k0 < g.Nx;
+    const bool act0 = j < g.Ny && k0 < g.Nx;
     const int Ny = g.Ny, Nz = g.Nz, px = g.px;
-    const int p = act ? (i * Ny + j) * px + k0 : 0;
+    const int p = act0 ? (i * Ny + j) * px + k0 : 0;
     const PmlAxis<T>& PX = g.pml[0];
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
-    const int ly = slab_local(PY, j, false);   // same for the whole warp
-    const int lz = slab_local(PZ, i + PZ.off, true);
+    const int ly0 = slab_local(PY, j, false);   // same for the whole warp
+    const int lz0 = slab_local(PZ, i + PZ.off, true);
+#ifdef FDTD_BOUNDS_CHECK
+    // a lane whose indices fall outside their arrays records the site and skips
+    const bool act = act0 && vecb::h_fields_ok(g, i, j, k0, lane, p);
+    const int ly = (ly0 >= 0 && act && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
+                                                      (long long)Nz * PY.wsum * px - V + 1, 5)) ? -1 : ly0;
+    const int lz = (lz0 >= 0 && act && !vecb::in_range(g, (long long)(lz0 * Ny + j) * px + k0, 0,
+                                                      (long long)PZ.wsum * Ny * px - V + 1, 6)) ? -1 : lz0;
+#else
+    const bool act = act0;
+    const int ly = ly0, lz = lz0;
+#endif
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
     const bool xs = xw && act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
@@ -131,6 +181,11 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
     for (int e = 0; e < V; e++) {
         const int k = k0 + e;
         lxs[e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
+#ifdef FDTD_BOUNDS_CHECK
+        if (lxs[e] >= 0 && !vecb::in_range(g, (long long)(i * Ny + j) * PX.wsum + lxs[e], 0,
+                                           (long long)Nz * Ny * PX.wsum, 7))
+            lxs[e] = -1;
+#endif
         if (lxs[e] >= 0) {
             const int s = (i * Ny + j) * PX.wsum + lxs[e];
             px0[e] = ld(PX.psi[0] + s); px1[e] = ld(PX.psi[1] + s);
@@ -222,14 +277,24 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
     constexpr unsigned FULL = 0xffffffffu;
     const int m = xb * 32 + lane;
     const int k0 = m * V;
-    const bool act = j < g.Ny && k0 < g.Nx;
+    const bool act0 = j < g.Ny && k0 < g.Nx;
     const int Ny = g.Ny, px = g.px;
-    const int p = act ? (i * Ny + j) * px + k0 : 0;
+    const int p = act0 ? (i * Ny + j) * px + k0 : 0;
     const PmlAxis<T>& PX = g.pml[0];
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
-    const int ly = slab_local(PY, j, false);   // same for the whole warp
-    const int lz = slab_local(PZ, i + PZ.off, true);
+    const int ly0 = slab_local(PY, j, false);   // same for the whole warp
+    const int lz0 = slab_local(PZ, i + PZ.off, true);
+#ifdef FDTD_BOUNDS_CHECK
+    const bool act = act0 && vecb::e_fields_ok(g, i, j, k0, lane, p);
+    const int ly = (ly0 >= 0 && act && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
+                                                      (long long)g.Nz * PY.wsum * px - V + 1, 15)) ? -1 : ly0;
+    const int lz = (lz0 >= 0 && act && !vecb::in_range(g, (long long)(lz0 * Ny + j) * px + k0, 0,
+                                                      (long long)PZ.wsum * Ny * px - V + 1, 16)) ? -1 : lz0;
+#else
+    const bool act = act0;
+    const int ly = ly0, lz = lz0;
+#endif
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
     const bool xs = xw && act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
@@ -265,6 +330,11 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
     for (int e = 0; e < V; e++) {
         const int k = k0 + e;
         lxs[e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
+#ifdef FDTD_BOUNDS_CHECK
+        if (lxs[e] >= 0 && !vecb::in_range(g, (long long)(i * Ny + j) * PX.wsum + lxs[e], 0,
+                                           (long long)g.Nz * Ny * PX.wsum, 17))
+            lxs[e] = -1;
+#endif
         if (lxs[e] >= 0) {
             const int s = (i * Ny + j) * PX.wsum + lxs[e];
             px2[e] = ld(PX.psi[2] + s); px3[e] = ld(PX.psi[3] + s);

@@ -17,7 +17,9 @@ import numpy as np
 from numpy.ctypeslib import ndpointer
 
 dir_path = os.path.dirname(os.path.realpath(__file__))
-so_path = os.path.join(dir_path, "FDTD.so")
+# EMOPT_B200_LIB selects another build of the library, e.g. FDTD_checked.so
+# (index-checked stepping kernels, for debugging)
+so_path = os.environ.get("EMOPT_B200_LIB") or os.path.join(dir_path, "FDTD.so")
 
 if not os.path.exists(so_path):
     raise ImportError(

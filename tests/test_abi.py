@@ -26,6 +26,21 @@ def test_library_exports_header_symbols():
     assert set(ct.REFERENCE_SYMBOLS) | set(ct.ADDED_SYMBOLS) == set(syms)
 
 
+def test_checked_library_exports_the_same_symbols():
+    """FDTD_checked.so (index-checked stepping kernels) is a drop-in for FDTD.so."""
+    from emopt_b200 import build
+    lib = ctypes.CDLL(build.CHECKED)
+    for s in header_symbols():
+        assert hasattr(lib, s), s
+    # EMOPT_B200_LIB selects it for the ctypes binding
+    import subprocess
+    import sys
+    code = "import emopt_b200.fdtd_ctypes as ct, os; print(os.path.basename(ct.so_path))"
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                         env=dict(os.environ, EMOPT_B200_LIB=build.CHECKED), timeout=300)
+    assert out.returncode == 0 and out.stdout.strip() == "FDTD_checked.so"
+
+
 def test_reference_binding_loads_unchanged():
     """The reference ctypes argtypes (emopt/fdtd_ctypes.py) bind to this library."""
     from emopt_b200 import fdtd_ctypes as ct
