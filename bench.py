@@ -53,7 +53,7 @@ def parse_args():
                     choices=["auto", "scalar", "fused_plain", "fused_tma", "fused_warp", "vector",
                              "vector16", "stream"])
     ap.add_argument("--workload", default="mmi",
-                    choices=["mmi", "waveguide", "serving", "grad", "grating", "zslab"])
+                    choices=["mmi", "waveguide", "serving", "grad", "grating", "zslab", "modes"])
     ap.add_argument("--slabs", type=int, default=2,
                     help="zslab on one process: z slabs on this GPU (under torchrun: one per rank)")
     ap.add_argument("--requests", type=int, default=512, help="serving: requests in the stream")
@@ -562,6 +562,92 @@ def run_zslab(args):
         dist.destroy_process_group()
 
 
+def run_modes(args):
+    """Mode-source generation: ModeFullVector.build + solve (4 modes nearest
+    n0 = 3.45) + get_source on the cross-section of the MMI block's input
+    waveguide (0.5 x 0.22 um silicon strip in oxide, 161 x 101 plane at
+    0.025 um: 97,566 unknowns), as the reference's mode-source set-up does it.
+    The oracle (the reference's matrices, SuperLU + ARPACK shift-and-invert)
+    is timed beside it on the host."""
+    import torch
+    from emopt_b200 import grid
+    from emopt_b200.misc import DomainCoordinates
+    from emopt_b200.modes import ModeFullVector
+    d, wl = 0.025, 1.55
+    Xs, Ys, Zs = 8.0, 4.0, 2.5
+    core = grid.Rectangle(Xs / 2, Ys / 2, 2 * Xs, 0.5)
+    core.layer, core.material_value = 1, 12.25
+    clad = grid.Rectangle(Xs / 2, Ys / 2, 2 * Xs, 2 * Ys)
+    clad.layer, clad.material_value = 2, 2.085
+    eps = grid.StructuredMaterial3D(Xs, Ys, Zs, d, d, d)
+    eps.add_primitive(clad, -Zs, Zs)
+    eps.add_primitive(core, Zs / 2 - 0.11, Zs / 2 + 0.11)
+    mu = grid.ConstantMaterial3D(1.0)
+    plane = DomainCoordinates.from_indices(100, 101, 0, 161, 0, 101, d, d, d)
+    times, applies = [], []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m = ModeFullVector(wl, eps, mu, plane, n0=3.45, neigs=4, device=0)
+        m.build()
+        m.solve()
+        src = m.get_source(0, d, d, d)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    # one operator application (B v, forward + backward sweep: the captured
+    # graph), device-timed
+    m._vin.copy_(torch.randn(m._NL * m._nb, dtype=torch.complex128, device="cuda"))
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        m._graph.replay()
+    reps = 20
+    e0.record(st)
+    for _ in range(reps):
+        m._graph.replay()
+    e1.record(st)
+    torch.cuda.synchronize()
+    apply_ms = e0.elapsed_time(e1) / reps
+    nb, NL, nr = m._nb, m._NL, int(m._rows.numel())
+    w_bytes = NL * (nr + nb) * nb * 16                  # every inverted block read once per sweep
+    peak = None
+    try:
+        peak = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                           "MEASURED_PEAKS.json")))["hbm_gbs"]
+        peak_kind = "measured"
+    except Exception:
+        peak, peak_kind = 6650.0, "fallback"
+    achieved = w_bytes / (apply_ms * 1e-3) / 1e9
+    med = statistics.median(times)
+    result = {
+        "metric": "mode solves/s (full-vector, 161x101 plane, 4 modes near n0=3.45, with get_source)",
+        "value": 1.0 / med, "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * med, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "mode_161x101_strip", "unknowns": 6 * 161 * 101, "lines": NL, "block": nb},
+        "neff": [complex(x).real for x in m.neff], "stats": m.stats,
+        "roofline": {"kernel": "k_line_gemv (one apply: %d launches)" % (2 * NL), "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "apply_ms": apply_ms, "bytes_per_apply": w_bytes},
+    }
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+        from oracle import modes as O
+        ef = lambda k, j, i: np.where((np.abs(j * d - Ys / 2) < 0.25) & (np.abs(i * d - Zs / 2) < 0.11),
+                                      12.25, 2.085) + 0j
+        mf = lambda k, j, i: np.ones(np.shape(k)) + 0j
+        t0 = time.perf_counter()
+        planes = O.material_planes(ef, mf, "x", 101, 161, 100, 0, 0)
+        A, B = O.build_system(planes, 101, 161, d, d, wl)
+        neff, V = O.solve(A, B, 3.45, 4)
+        tc = time.perf_counter() - t0
+        result["cpu_baseline"] = {"value": 1.0 / tc, "unit": "solves/s", "cores": 1, "kind": "port",
+                                  "sample": "one solve of the same plane (SuperLU + ARPACK, 4 modes)",
+                                  "neff": [complex(x).real for x in neff]}
+    print(json.dumps(result), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -574,6 +660,8 @@ def main():
         run_grating(args)
     elif args.workload == "zslab":
         run_zslab(args)
+    elif args.workload == "modes":
+        run_modes(args)
     else:
         run_ours(args)
 

@@ -199,6 +199,31 @@ libFDTD.FDTD_structured_values.argtypes = [c_int, c_void_p, c_void_p, c_int, c_v
                                            c_void_p, c_char_p, c_int]
 libFDTD.FDTD_structured_values.restype = c_int
 
+
+class ModeLines(Structure):
+    """FDTDModeLines: the plane's M x N points cut into lines (rows of
+    constant y when sweep_y, else columns of constant x)."""
+    _fields_ = [("M", c_int), ("N", c_int), ("sweep_y", c_int)]
+
+
+libFDTD.FDTD_mode_last_error.argtypes = []
+libFDTD.FDTD_mode_last_error.restype = c_char_p
+libFDTD.FDTD_mode_assemble.argtypes = [c_void_p, c_int, c_void_p, c_double, c_double, c_double,
+                                       c_double, c_double, c_void_p, c_char_p, c_void_p, c_void_p,
+                                       c_void_p, c_void_p, c_void_p]
+libFDTD.FDTD_mode_assemble.restype = c_int
+libFDTD.FDTD_mode_schur.argtypes = [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                    c_void_p, c_void_p]
+libFDTD.FDTD_mode_schur.restype = c_int
+libFDTD.FDTD_mode_apply.argtypes = [c_void_p, c_int, c_void_p, c_double, c_void_p, c_void_p, c_void_p,
+                                    c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p,
+                                    c_void_p, c_void_p]
+libFDTD.FDTD_mode_apply.restype = c_int
+libFDTD.FDTD_mode_source.argtypes = [c_int, c_void_p, c_int, c_int, c_void_p, c_double, c_double,
+                                     c_double, c_double, c_double, c_double, c_double, c_void_p,
+                                     c_void_p, c_void_p, c_char_p, c_void_p]
+libFDTD.FDTD_mode_source.restype = c_int
+
 ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_zchunk",
                  "FDTD_set_precision", "FDTD_set_kernel", "FDTD_solve_cw",
                  "FDTD_amp_phase_noalloc", "FDTD_grad_eps", "FDTD_serve_new",
@@ -207,7 +232,8 @@ ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_
                  "FDTD_serve_delete", "FDTD_set_stream", "FDTD_slab_set", "FDTD_slab_begin",
                  "FDTD_slab_step", "FDTD_slab_halo", "FDTD_slab_sample", "FDTD_slab_probe",
                  "FDTD_slab_capture", "FDTD_slab_finish", "FDTD_structured_values",
-                 "FDTD_host_register", "FDTD_host_unregister")
+                 "FDTD_host_register", "FDTD_host_unregister", "FDTD_mode_last_error",
+                 "FDTD_mode_assemble", "FDTD_mode_schur", "FDTD_mode_apply", "FDTD_mode_source")
 
 
 class FDTDError(RuntimeError):

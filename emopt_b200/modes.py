@@ -1,0 +1,446 @@
+"""Full-vector waveguide modes on the GPU: ``ModeFullVector`` of the reference
+(emopt/modes.py:1099-2298) with the same constructor, properties and
+methods, so that a mode source or a mode-match field comes from the device.
+
+The reference assembles the 6 M N x 6 M N system A x = n B x of the plane's
+six field components (emopt/modes.py:1278-1588) and solves it with SLEPc,
+shift-and-invert about the target ``n0``, factoring ``A - n0 B`` with MUMPS.
+Here the same rows are assembled on the GPU into a block-tridiagonal matrix
+(the plane cut into lines; ``emopt_b200/csrc/modes.cu``), the Schur
+complements of its block LU are inverted on the device, and a Krylov-Schur
+iteration (Stewart, SIAM J. Matrix Anal. Appl. 23 (2001) 601-614) on
+``(A - n0 B)^-1 B`` finds the eigenvalues theta of largest modulus, i.e. the
+effective indices ``n = n0 + 1/theta`` closest to ``n0``, closest first (the
+order SLEPc returns with a target).  Every application of the operator is a
+forward and a backward sweep of dense matrix-vector products over the
+inverted blocks, HBM-bound.
+
+Eigenvectors are normalised to unit 2-norm with their entry of largest
+modulus real and positive (SLEPc's phase follows its random start vector;
+any phase is a valid mode).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import scipy.linalg as sla
+
+from . import fdtd_ctypes as _ct
+from .fdtd_ctypes import libFDTD
+from .grid import Material3D
+from .misc import warning_message
+
+COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+_PERMUTE = {"x": {"Ex": "Ez", "Ey": "Ex", "Ez": "Ey", "Hx": "Hz", "Hy": "Hx", "Hz": "Hy"},
+            "y": {"Ex": "Ey", "Ey": "Ez", "Ez": "Ex", "Hx": "Hy", "Hy": "Hz", "Hz": "Hx"},
+            "z": {c: c for c in COMPONENTS}}
+_BCS = ("0", "M", "E", "H", "P", "EM", "HM")
+
+
+def _check(rc, what):
+    if rc != _ct.FDTD_OK:
+        raise _ct.FDTDError("%s: %s" % (what, libFDTD.FDTD_mode_last_error().decode()))
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class ModeFullVector:
+    """Modes of a 2D slice of a 3D structure (emopt/modes.py:1099-1276).
+
+    Parameters as the reference: ``wavelength``, ``eps`` and ``mu``
+    (Material3D), ``domain`` (a plane: one of its three sizes is 1), ``n0``
+    (the effective index the modes are sought near), ``neigs``,
+    ``backwards``, ``verbose``.  Additions: ``device`` (CUDA device index)
+    and ``sweep`` ('y' or 'x': the lines of the block-tridiagonal solve; by
+    default the shorter of the plane's two directions).
+    """
+
+    def __init__(self, wavelength, eps, mu, domain, n0=1.0, neigs=1, backwards=False, verbose=True,
+                 device=None, sweep=None):
+        import torch
+        self._neff = np.zeros(neigs, dtype=np.complex128)
+        self.n0 = n0
+        self.neigs = neigs
+        self.wavelength = wavelength
+        self.eps, self.mu, self.domain = eps, mu, domain
+        self._fshape = domain.shape
+        if domain.Nx == 1:
+            self.ndir, self._M, self._N, self.dx, self.dy = "x", domain.Nz, domain.Ny, domain.dy, domain.dz
+        elif domain.Ny == 1:
+            self.ndir, self._M, self._N, self.dx, self.dy = "y", domain.Nz, domain.Nx, domain.dx, domain.dz
+        elif domain.Nz == 1:
+            self.ndir, self._M, self._N, self.dx, self.dy = "z", domain.Ny, domain.Nx, domain.dx, domain.dy
+        else:
+            raise AttributeError("3D domains are not supported for 2D mode calculations!")
+        self.verbose = verbose
+        self._dir = -1.0 if backwards else 1.0
+        self.R = self.wavelength / (2 * np.pi)
+        self._bc = ["0", "0"]
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self._dev = torch.device("cuda", self.device)
+        if sweep is None:
+            sweep = "y" if self._N <= self._M else "x"
+        if sweep not in ("x", "y"):
+            raise ValueError("sweep must be 'x' or 'y'")
+        self._lines = _ct.ModeLines(self._M, self._N, 1 if sweep == "y" else 0)
+        self._planes = None
+        self._x = None
+        self.stats = {}
+
+    # ------------------------------------------------------------ attributes
+    @property
+    def neff(self):
+        return self._neff
+
+    @neff.setter
+    def neff(self, value):
+        warning_message("neff cannot be set by the user.", module="emopt_b200.modes")
+
+    @property
+    def bc(self):
+        return self._bc
+
+    @bc.setter
+    def bc(self, bc):
+        for b in bc[:2]:
+            if b not in _BCS:
+                raise ValueError("Boundary condition type '%s' not found. Use 0, M, E, H, P, EM, HM." % b)
+        self._bc = list(bc)
+
+    def _bc_code(self):
+        """The two boundary letters the kernels test ('0', 'E', 'H'; the other
+        types change no row of the reference's system)."""
+        return "".join(b if b in ("0", "E", "H") else "-" for b in self._bc[:2]).encode()
+
+    # --------------------------------------------------------------- build
+    def _values(self, mat, k1, k2, j1, j2, i1, i2, sx=0.0, sy=0.0, sz=0.0):
+        import torch
+        try:
+            v = mat.get_values(k1, k2, j1, j2, i1, i2, sx, sy, sz, device=self._dev)
+        except TypeError:
+            v = mat.get_values(k1, k2, j1, j2, i1, i2, sx, sy, sz)
+        return torch.as_tensor(v, dtype=torch.complex128, device=self._dev)
+
+    def _material_planes(self):
+        """eps_x, eps_y, eps_z, mu_x, mu_y, mu_z as ModeFullVector.build samples
+        them for a Material3D (emopt/modes.py:1327-1352), [M][N] each."""
+        if not isinstance(self.eps, Material3D) or not isinstance(self.mu, Material3D):
+            raise TypeError("the GPU mode solver takes Material3D slices")
+        d, M, N = self.domain, self._M, self._N
+        k0, j0, i0 = d.k1, d.j1, d.i1
+        out = []
+        if self.ndir == "x":
+            offs = [(self.eps, 0.5, -0.5), (self.eps, 0.0, 0.0), (self.eps, 0.0, -0.5),
+                    (self.mu, 0.0, 0.0), (self.mu, 0.5, -0.5), (self.mu, 0.5, 0.0)]
+            for mat, sy, sz in offs:
+                out.append(self._values(mat, k0, k0 + 1, j0, j0 + N, i0, i0 + M, 0.0, sy, sz)[:, :, 0])
+        elif self.ndir == "y":
+            # the reference's lambdas put the plane's x along z and its y along x
+            offs = [(self.eps, 0.0, 0.0), (self.eps, 0.5, -0.5), (self.eps, 0.0, -0.5),
+                    (self.mu, 0.5, -0.5), (self.mu, 0.0, 0.0), (self.mu, 0.5, 0.0)]
+            for mat, sx, sz in offs:
+                out.append(self._values(mat, k0, k0 + M, j0, j0 + 1, i0, i0 + N, sx, 0.0, sz)[:, 0, :].T)
+        else:
+            for mat in (self.eps,) * 3 + (self.mu,) * 3:
+                out.append(self._values(mat, k0, k0 + N, j0, j0 + M, i0, i0 + 1)[0])
+        return [p.contiguous() for p in out]
+
+    def build(self):
+        """Sample the materials on the plane (the reference assembles A and B
+        here; the GPU blocks depend on the target and are assembled in
+        :meth:`solve`)."""
+        self._planes = self._material_planes()
+
+    # --------------------------------------------------------------- solve
+    def _factor(self, sigma):
+        import torch
+        g, dev = self._lines, self._dev
+        L = self._N if g.sweep_y else self._M
+        NL = self._M if g.sweep_y else self._N
+        nb = 6 * L
+        self._L, self._NL, self._nb = L, NL, nb
+        D = torch.empty((NL, nb, nb), dtype=torch.complex128, device=dev)
+        pcol = torch.empty((NL, nb), dtype=torch.int32, device=dev)
+        ncol = torch.empty((NL, nb), dtype=torch.int32, device=dev)
+        pval = torch.empty((NL, nb), dtype=torch.complex128, device=dev)
+        nval = torch.empty((NL, nb), dtype=torch.complex128, device=dev)
+        planes = (ctypes.c_void_p * 6)(*[p.data_ptr() for p in self._planes])
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        odx, ody = self.R / self.dx, self.R / self.dy
+        _check(libFDTD.FDTD_mode_assemble(ctypes.byref(g), self.device, stream, odx, ody, self._dir,
+                                          float(np.real(sigma)), float(np.imag(sigma)), planes,
+                                          self._bc_code(), _ptr(D),
+                                          _ptr(pcol), _ptr(pval), _ptr(ncol), _ptr(nval)),
+               "FDTD_mode_assemble")
+        # every column of line l that a row of line l - 1 reaches is reached once
+        nc = ncol.cpu().numpy()
+        for l in range(NL):
+            c = nc[l][nc[l] >= 0]
+            if len(np.unique(c)) != len(c):
+                raise RuntimeError("line couplings are not one to one")
+        for l in range(NL):
+            if l > 0:
+                _check(libFDTD.FDTD_mode_schur(ctypes.byref(g), self.device, stream, l, _ptr(D), _ptr(pcol),
+                                               _ptr(pval), _ptr(ncol), _ptr(nval)), "FDTD_mode_schur")
+            W, info = torch.linalg.inv_ex(D[l])
+            if int(info) != 0:
+                raise RuntimeError("A - n0 B is singular on line %d: move n0 off the eigenvalue" % l)
+            D[l].copy_(W)
+        rows = torch.unique(pcol[pcol >= 0]).to(torch.int32)
+        self._W, self._pcol, self._pval, self._ncol, self._nval, self._rows = D, pcol, pval, ncol, nval, rows
+        n = NL * nb
+        self._rhs = torch.empty(n, dtype=torch.complex128, device=dev)
+        self._h = torch.empty(n, dtype=torch.complex128, device=dev)
+
+    def _apply_direct(self, v, out):
+        import torch
+        stream = torch.cuda.current_stream(self._dev).cuda_stream
+        _check(libFDTD.FDTD_mode_apply(ctypes.byref(self._lines), self.device, stream, self._dir, _ptr(self._W),
+                                       _ptr(self._pcol), _ptr(self._pval), _ptr(self._ncol), _ptr(self._nval),
+                                       _ptr(self._rows), int(self._rows.numel()), _ptr(v), 1, _ptr(self._rhs),
+                                       _ptr(self._h), _ptr(out)), "FDTD_mode_apply")
+        return out
+
+    def _capture(self):
+        """One application of (A - n0 B)^-1 B (2 NL sweep launches) as a CUDA
+        graph on fixed buffers, replayed by :meth:`_apply`."""
+        import torch
+        n = self._NL * self._nb
+        self._vin = torch.zeros(n, dtype=torch.complex128, device=self._dev)
+        self._xout = torch.empty(n, dtype=torch.complex128, device=self._dev)
+        self._apply_direct(self._vin, self._xout)          # outside the capture first
+        torch.cuda.synchronize(self._dev)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._apply_direct(self._vin, self._xout)
+        self._graph = g
+
+    def _apply(self, v, out):
+        self._vin.copy_(v)
+        self._graph.replay()
+        out.copy_(self._xout)
+        return out
+
+    def _to_solver_order(self, X):
+        """[k][NL*nb] line order -> [k][6][M][N]."""
+        k = X.shape[0]
+        Y = X.view(k, self._NL, 6, self._L)
+        if self._lines.sweep_y:                       # [k][y][c][x]
+            return Y.permute(0, 2, 1, 3).contiguous()
+        return Y.permute(0, 2, 3, 1).contiguous()     # [k][x][c][y] -> [k][c][y][x]
+
+    def solve(self, tol=1e-12, maxit=100, ncv=None, seed=0):
+        """Solve for the ``neigs`` modes closest to ``n0``."""
+        import time
+
+        import torch
+        if self._planes is None:
+            self.build()
+        t0 = time.perf_counter()
+        sigma = complex(self.n0)
+        self._factor(sigma)
+        self._capture()
+        torch.cuda.synchronize(self._dev)
+        t1 = time.perf_counter()
+        k = self.neigs
+        m = ncv or max(3 * k, k + 20)
+        n = self._NL * self._nb
+        m = min(m, n - 1)
+        rng = np.random.default_rng(seed)
+        v0 = torch.as_tensor(rng.standard_normal(n) + 1j * rng.standard_normal(n), device=self._dev)
+        theta, X, nconv, napply = _krylov_schur(self._apply, n, k, m, tol, maxit, v0, self._dev)
+        torch.cuda.synchronize(self._dev)
+        t2 = time.perf_counter()
+        if nconv < k:
+            warning_message("%d eigenmodes were requested, however only %d eigenmodes were found."
+                            % (k, nconv), module="emopt_b200.modes")
+        F = self._to_solver_order(X)
+        # unit 2-norm, the entry of largest modulus real and positive
+        flat = F.view(F.shape[0], -1)
+        flat /= torch.linalg.vector_norm(flat, dim=1, keepdim=True)
+        big = flat.gather(1, flat.abs().argmax(dim=1, keepdim=True))
+        flat *= (big.abs() / big)
+        self._x = F
+        self._neff = np.zeros(k, dtype=np.complex128)
+        self._neff[:len(theta)] = sigma + 1.0 / np.asarray(theta)
+        self.stats = {"factor_s": t1 - t0, "iterate_s": t2 - t1, "applications": napply,
+                      "lines": self._NL, "block": self._nb}
+
+    # ----------------------------------------------------------- the fields
+    def _raw(self, i, component):
+        q = COMPONENTS.index(component)
+        return self._x[i, q]
+
+    def get_field(self, i, component, permute=True, squeeze=False):
+        """Raw field component of mode i (emopt/modes.py:1651-1787)."""
+        if permute:
+            component = _PERMUTE[self.ndir][component]
+        f = self._raw(i, component).cpu().numpy()
+        return f if squeeze else np.reshape(f, self._fshape)
+
+    def get_field_interp(self, i, component, squeeze=False):
+        """Field component of mode i averaged onto the plane's Ez-equivalent
+        points (emopt/modes.py:1789-2052; the y-normal Ex and Hy, which fail
+        in the reference, give the raw field)."""
+        f = np.pad(self.get_field(i, component, squeeze=True), 1, "constant", constant_values=0)
+        c = _PERMUTE[self.ndir][component]
+        b0, b1 = self._bc[0], self._bc[1]
+
+        def gx(a):                      # x ghost column by the first boundary
+            if b0 == "E":
+                a[:, 0] = -1 * a[:, 1]
+            elif b0 == "H":
+                a[:, 0] = a[:, 1]
+
+        def gy(a):
+            if b1 == "E":
+                a[0, :] = -1 * a[1, :]
+            elif b1 == "H":
+                a[0, :] = a[1, :]
+
+        g = np.copy(f)
+        if self.ndir == "x":
+            if c in ("Ex", "Hy"):
+                gx(f); g[:, 1:] += f[:, :-1]; g[:-1, 1:] += f[1:, :-1]; g[:-1, :] += f[1:, :]; out = g / 4.0
+            elif c in ("Ey", "Hx"):
+                out = f
+            elif c == "Ez":
+                g[:-1, :] += g[1:, :]; out = g / 2.0
+            else:
+                gx(f); g[:, 1:] += f[:, :-1]; out = g / 2.0
+        elif self.ndir == "y":
+            if c in ("Ex", "Hy"):
+                out = f
+            elif c in ("Ey", "Hx"):
+                gy(f); g[:, :-1] += g[:, 1:]; g[1:, :] += g[:-1, :]; g[1:, :-1] += g[:-1, 1:]; out = g / 4.0
+            elif c == "Ez":
+                g[:, :-1] += g[:, 1:]; out = g / 2.0
+            else:
+                gy(f); g[1:, :] += f[:-1, :]; out = g / 2.0
+        else:
+            if c in ("Ex", "Hy"):
+                gx(f); g[:, 1:] += f[:, :-1]; out = g / 2.0
+            elif c in ("Ey", "Hx"):
+                gy(f); g[1:, :] += f[:-1, :]; out = g / 2.0
+            elif c == "Ez":
+                out = f
+            else:
+                gy(f); gx(f); g[:, 1:] += f[:, :-1]; g[1:, :] += f[:-1, :]; g[1:, 1:] += f[:-1, :-1]; out = g / 4.0
+        out = out[1:-1, 1:-1]
+        return out if squeeze else np.reshape(out, self._fshape)
+
+    def component_energy(self, i):
+        """Fractions of the mode's energy in Ex..Hz (emopt/modes.py:2054-2097)."""
+        eps = np.asarray(self.eps.get_values_in(self.domain, squeeze=True)).real
+        mu = np.asarray(self.mu.get_values_in(self.domain, squeeze=True)).real
+        W = [np.sum((eps if c[0] == "E" else mu) * np.abs(self.get_field(i, c, squeeze=True)) ** 2)
+             for c in COMPONENTS]
+        tot = sum(W)
+        return [w / tot for w in W]
+
+    def get_mode_number(self, i):
+        raise NotImplementedError("mode numbering is not implemented (it is a stub in the reference)")
+
+    def find_mode_index(self, P, Q):
+        for i in range(self.neigs):
+            p, q = self.get_mode_number(i)
+            if p == P and q == Q:
+                return i
+        warning_message("Desired mode number was not found.", "emopt_b200.modes")
+        return 0
+
+    def get_source(self, i, dx, dy, dz):
+        """(Jx, Jy, Jz, Mx, My, Mz) that launch mode i (emopt/modes.py:2144-2296),
+        each shaped like the domain, in the caller's axes."""
+        import torch
+        if not isinstance(self.eps, Material3D):
+            raise Exception("Source calculation only possible for slices of Material3D's..")
+        d = self.domain
+        if self.ndir == "x":
+            mydx, mydy, mydz = dy, dz, dx
+            mu05 = self._values(self.mu, d.k1, d.k2, d.j1, d.j2, d.i1, d.i2, 0.0, 0.0, 0.5)[:, :, 0]
+            mu50 = self._values(self.mu, d.k1, d.k2, d.j1, d.j2, d.i1, d.i2, 0.0, 0.5, 0.0)[:, :, 0]
+        elif self.ndir == "y":
+            mydx, mydy, mydz = dz, dx, dy
+            mu05 = self._values(self.mu, d.k1, d.k2, d.j1, d.j2, d.i1, d.i2, 0.0, 0.0, 0.5)[:, 0, :]
+            mu50 = self._values(self.mu, d.k1, d.k2, d.j1, d.j2, d.i1, d.i2, 0.5, 0.0, 0.0)[:, 0, :]
+        else:
+            mydx, mydy, mydz = dx, dy, dz
+            mu05 = self._values(self.mu, d.k1, d.k2, d.j1, d.j2, d.i1, d.i2, 0.0, 0.5, 0.0)[0]
+            mu50 = self._values(self.mu, d.k1, d.k2, d.j1, d.j2, d.i1, d.i2, 0.5, 0.0, 0.0)[0]
+        eps = self._values(self.eps, d.k1, d.k2, d.j1, d.j2, d.i1, d.i2).reshape(self._M, self._N).contiguous()
+        mu05, mu50 = mu05.contiguous(), mu50.contiguous()
+        neff = complex(self._neff[i])
+        dxn, dyn, dzn = mydx / self.R, mydy / self.R, mydz / self.R
+        ekz = np.exp(1j * self._dir * neff * dzn / 2)
+        F = self._x[i]
+        S = complex(0.5 * mydx * mydy * torch.sum(F[0] * F[4].conj() - F[1] * F[3].conj()).item())
+        s = 1.0 / np.sqrt(S)
+        out = torch.empty((6, self._M, self._N), dtype=torch.complex128, device=self._dev)
+        stream = torch.cuda.current_stream(self._dev).cuda_stream
+        bc = self._bc_code()
+        _check(libFDTD.FDTD_mode_source(self.device, stream, self._M, self._N, _ptr(F), s.real, s.imag,
+                                        ekz.real, ekz.imag, dxn, dyn, dzn, _ptr(eps), _ptr(mu05), _ptr(mu50),
+                                        bc, _ptr(out)), "FDTD_mode_source")
+        Jx, Jy, Jz, Mx, My, Mz = (np.reshape(a, self._fshape) for a in out.cpu().numpy())
+        if self.ndir == "x":
+            return Jz, Jx, Jy, Mz, Mx, My
+        if self.ndir == "y":
+            return Jy, Jz, Jx, My, Mz, Mx
+        return Jx, Jy, Jz, Mx, My, Mz
+
+
+def _krylov_schur(apply, n, k, m, tol, maxit, v0, dev):
+    """Krylov-Schur iteration for the k eigenvalues of largest modulus of the
+    operator ``apply`` (n x n, device vectors), m-dimensional subspace.
+    Returns (theta[k'], vectors[k'][n], k' converged, applications)."""
+    import torch
+    V = torch.empty((m + 1, n), dtype=torch.complex128, device=dev)
+    H = np.zeros((m + 1, m), dtype=np.complex128)
+    V[0] = v0 / torch.linalg.vector_norm(v0)
+    w = torch.empty(n, dtype=torch.complex128, device=dev)
+    p, napply = 0, 0
+    theta = S = order = None
+    for _ in range(maxit):
+        for j in range(p, m):
+            apply(V[j], w)
+            napply += 1
+            Vj = V[:j + 1]
+            h = Vj.conj() @ w                      # classical Gram-Schmidt, twice
+            w -= h @ Vj
+            h2 = Vj.conj() @ w
+            w -= h2 @ Vj
+            h += h2
+            beta = float(torch.linalg.vector_norm(w))
+            H[:j + 1, j] = h.cpu().numpy()
+            H[j + 1, j] = beta
+            if beta == 0.0:
+                m = j + 1
+                break
+            V[j + 1] = w / beta
+        Hm = H[:m, :m]
+        theta, S = np.linalg.eig(Hm)
+        order = np.argsort(-np.abs(theta))
+        res = np.abs(H[m, m - 1] * S[m - 1, :])
+        done = [res[q] <= tol * abs(theta[q]) for q in order[:k]]
+        if all(done) or H[m, m - 1] == 0:
+            break
+        keep = min(m - 1, max(k + (m - k) // 2, k + 1))
+        thr = np.abs(theta[order[keep - 1]])
+        T, Z, sdim = sla.schur(Hm, output="complex", sort=lambda z: abs(z) >= thr * (1 - 1e-12))
+        p = int(min(max(sdim, k), m - 1))
+        Zt = torch.as_tensor(np.ascontiguousarray(Z[:, :p].T), device=dev)
+        V[:p] = Zt @ V[:m]
+        V[p] = V[m]
+        Hn = np.zeros_like(H)
+        Hn[:p, :p] = T[:p, :p]
+        Hn[p, :p] = H[m, m - 1] * Z[m - 1, :p]
+        H = Hn
+    res = np.abs(H[m, m - 1] * S[m - 1, :])
+    good = [q for q in order[:k] if res[q] <= max(tol, 1e-8) * abs(theta[q])]
+    Sk = torch.as_tensor(np.ascontiguousarray(S[:, good].T), device=dev)
+    X = Sk @ V[:m]
+    return theta[good], X, len(good), napply

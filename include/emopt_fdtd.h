@@ -337,6 +337,61 @@ int FDTD_structured_values(int device, void *stream, const double *zs, int nzs,
                            int k1, int k2, int j1, int j2, int i1, int i2, double sx, double sy,
                            double sz, fdtd_complex128 *out, char *msg, int msglen);
 
+/* ---- full-vector waveguide modes (replaces the SLEPc/MUMPS solve of the
+ * reference's ModeFullVector, emopt/modes.py:1099-2298, which assembles
+ * A x = n B x with PETSc and solves it by shift-and-invert about n0).
+ * The plane (M rows of N points; row y, column x) is cut into lines: rows of
+ * constant y when sweep_y, else columns of constant x.  A line of L points
+ * holds nb = 6 L unknowns (Ex Ey Ez Hx Hy Hz blocks of L), NL lines in all;
+ * vectors are complex128 in line order ((l * 6 + c) * L + p).  All pointers
+ * are device memory; complex values are interleaved (re, im) doubles.  The
+ * dense inverses of the Schur complements are the caller's (a device LU):
+ * after FDTD_mode_assemble, for l = 0, 1, ...: FDTD_mode_schur(l) (l >= 1),
+ * then replace block l of D by its inverse. */
+typedef struct FDTDModeLines {
+    int M, N;
+    int sweep_y;
+} FDTDModeLines;
+
+/* Message of the last failing FDTD_mode_* call of this host thread. */
+const char *FDTD_mode_last_error(void);
+
+/* Blocks D_l of A - sigma B (emopt/modes.py:1361-1585; D: NL x nb x nb) and
+ * the couplings of each row to the lines before and after (pcol/ncol: column
+ * in that line or -1; pval/nval: the coefficient; NL x nb each).  planes[6]:
+ * eps_x eps_y eps_z mu_x mu_y mu_z on the plane ([M][N] complex128, sampled
+ * where the reference's build samples them); bc: the plane's two boundary
+ * letters; odx, ody: wavelength/(2 pi) over the spacings; dir: +1, or -1 for
+ * a backward mode. */
+int FDTD_mode_assemble(const FDTDModeLines *g, int device, void *stream, double odx, double ody,
+                       double dir, double sigma_re, double sigma_im, const double *const *planes,
+                       const char *bc, double *D, int *pcol, double *pval, int *ncol, double *nval);
+
+/* Schur complement of line l >= 1 in place: D_l -= L_l D_{l-1} U_{l-1}, with
+ * D_{l-1} already replaced by its inverse. */
+int FDTD_mode_schur(const FDTDModeLines *g, int device, void *stream, int l, double *D,
+                    const int *pcol, const double *pval, const int *ncol, const double *nval);
+
+/* x = (A - sigma B)^-1 (B v) (apply_b) or (A - sigma B)^-1 v, with W the
+ * inverted blocks: a forward and a backward sweep over the lines.  rows[nrows]:
+ * the local columns that rows of the next line reference (every pcol value);
+ * rhs, h: NL x nb scratch; x: NL x nb. */
+int FDTD_mode_apply(const FDTDModeLines *g, int device, void *stream, double dir, const double *W,
+                    const int *pcol, const double *pval, const int *ncol, const double *nval,
+                    const int *rows, int nrows, const double *v, int apply_b, double *rhs, double *h,
+                    double *x);
+
+/* Current sources of a mode (ModeFullVector.get_source, emopt/modes.py:2144-
+ * 2296) from its six raw field planes (fields: [6][M][N], solver order):
+ * scaled by s = 1/sqrt(S), ekz = exp(i dir neff dz/2); dxn, dyn, dzn: the
+ * non-dimensional spacings along the plane's axes and its normal; eps, mu05,
+ * mu50: [M][N] material planes; out: [6][M][N] Jx Jy Jz Mx My Mz in the
+ * plane's own axes. */
+int FDTD_mode_source(int device, void *stream, int M, int N, const double *fields, double s_re,
+                     double s_im, double ekz_re, double ekz_im, double dxn, double dyn, double dzn,
+                     const double *eps, const double *mu05, const double *mu50, const char *bc,
+                     double *out);
+
 #ifdef __cplusplus
 }
 #endif
