@@ -39,7 +39,7 @@ def _layered(M, N, seed):
 
 @pytest.mark.parametrize("bc,back", [(("0", "0"), False), (("E", "H"), True), (("H", "E"), False)])
 def test_shift_invert_matches_dense(bc, back):
-    M, N = 10, 12
+    M, N = 8, 11
     A, B = O.build_system(_layered(M, N, 1), M, N, 0.05, 0.06, WL, bc=bc, backwards=back)
     w1, V1 = O.solve(A, B, 3.3, 4)
     w2, V2 = O.solve_dense(A, B, 3.3, 4)
