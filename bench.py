@@ -609,8 +609,10 @@ def run_modes(args):
     e1.record(st)
     torch.cuda.synchronize()
     apply_ms = e0.elapsed_time(e1) / reps
-    nb, NL, nr = m._nb, m._NL, int(m._rows.numel())
-    w_bytes = NL * (nr + nb) * nb * 16                  # every inverted block read once per sweep
+    nb, NL, nq = m._nb, m._NL, int(m._QpQn32.numel())
+    # every inverted block read once by the back-substitution, its coupling
+    # rows once more by the reduction (all lines but the top one)
+    w_bytes = ((NL - 1) * nq + NL * nb) * nb * 16
     peak = None
     try:
         peak = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
@@ -627,7 +629,7 @@ def run_modes(args):
         "dtype": "c128", "data": "synthetic",
         "config": {"workload": "mode_161x101_strip", "unknowns": 6 * 161 * 101, "lines": NL, "block": nb},
         "neff": [complex(x).real for x in m.neff], "stats": m.stats,
-        "roofline": {"kernel": "k_line_gemv (one apply: %d launches)" % (2 * NL), "bound": "hbm",
+        "roofline": {"kernel": "k_lines_gemv (one apply: %d reduction levels)" % m.stats_levels, "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "apply_ms": apply_ms, "bytes_per_apply": w_bytes},
     }

@@ -8,18 +8,18 @@
 // block-tridiagonal matrix: the plane is cut into lines (rows of constant y,
 // or columns of constant x, whichever are shorter), every unknown of a line
 // couples only to its own line and the two lines beside it, so A - n0 B is
-// block tridiagonal with blocks of 6 L (L = the line length).  Its block LU
-// keeps the inverses W_l = S_l^-1 of the Schur complements
-//   S_0 = D_0,  S_l = D_l - L_l W_{l-1} U_{l-1},
-// and one application of (A - n0 B)^-1 is a forward and a backward sweep of
-// dense matrix-vector products with the W_l (HBM-bound: every W_l is read
-// once per sweep) plus the sparse couplings between lines (each row of the
-// system has at most one entry in the previous and one in the next line).
+// block tridiagonal with blocks of 6 L (L = the line length), each row with
+// at most one entry in the previous and one in the next line.  The caller
+// (emopt_b200/modes.py) factors it by block cyclic reduction -- batched
+// inverses of the lines eliminated at each level, and dense corrections on
+// the 2L x 2L coupling blocks -- and one application of (A - n0 B)^-1 is a
+// reduction and a back-substitution over the levels, each level one batched
+// matrix-vector product over the inverted blocks of its lines (HBM-bound:
+// every inverted block is read once per application, the reduction reading
+// only the rows the neighbouring lines couple to).
 //
 // Vectors on the device are in line order: index (l * 6 + c) * L + p for
 // line l, component c (Ex Ey Ez Hx Hy Hz) and position p along the line.
-// The dense inverses themselves are computed by the caller (a library LU on
-// the device); everything else is here.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -182,24 +182,6 @@ __global__ void k_assemble(Lines G, double odx, double ody, double dir, C2 sigma
     }
 }
 
-// S_l -= L_l W_{l-1} U_{l-1}: for each row r of line l with an entry in line
-// l-1 (column a) and each row b of line l-1 with an entry in line l
-// (column c): S_l[r][c] -= pval[r] W[a][b] nval[b].  One thread per (r, b);
-// the columns c of distinct b are distinct (checked on the host), so no two
-// threads write one element.
-__global__ void k_schur(int nb, double* S, const double* Wprev, const int* pcol, const double* pval,
-                        const int* ncol_prev, const double* nval_prev) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)nb * nb) return;
-    const int r = (int)(t / nb), b = (int)(t % nb);
-    const int a = pcol[r], c = ncol_prev[b];
-    if (a < 0 || c < 0) return;
-    const C2 w = ld2(Wprev + 2 * ((long long)a * nb + b));
-    const C2 d = ld2(pval + 2 * r) * w * ld2(nval_prev + 2 * b);
-    double* s = S + 2 * ((long long)r * nb + c);
-    st2(s, ld2(s) - d);
-}
-
 // out = B v (line order).
 __global__ void k_bmul(Lines G, double dir, const double* v, double* out) {
     const long long n = (long long)G.NL * G.nb;
@@ -213,35 +195,37 @@ __global__ void k_bmul(Lines G, double dir, const double* v, double* out) {
     }
 }
 
-// One line of a sweep: out[a] += sum_b W[a][b] v[b] over one tile of
-// GEMV_COLS columns, for the rows a listed in `rows` (all rows when rows is
-// null), where
-//   v = rhs - pval * hprev[pcol] - nval * xnext[ncol]
-// (terms with a null vector left out) is staged in shared memory for the
-// tile.  A CTA covers 8 rows (a warp each) of one column tile; every lane
-// issues its GEMV_COLS/32 loads of the row before it reduces, and the partial
-// sums of the column tiles meet in `out` (zeroed by the caller) by atomic adds.
+// Batched over lines: for each line l = lines[z] (blockIdx.z),
+//   out_l[a] += sum_b W_l[a][b] (rhs_l[b] - corr_l[b])
+// for the rows a listed in `rows` (all nb rows when rows is null), over one
+// tile of GEMV_COLS columns (blockIdx.x); corr may be null.  The tile of the
+// vector is staged in shared memory; a CTA covers 8 rows (a warp each), every
+// lane issues its GEMV_COLS/32 loads of the row before it reduces, and the
+// partial sums of the column tiles meet in `out` (zeroed by the caller) by
+// atomic adds.
 constexpr int GEMV_COLS = 256;
 
-__global__ void __launch_bounds__(256) k_line_gemv(int nb, const double* W, const int* rows, int nrows,
-                                                   const double* rhs, const int* pcol, const double* pval,
-                                                   const double* hprev, const int* ncol, const double* nval,
-                                                   const double* xnext, double* out) {
+__global__ void __launch_bounds__(256) k_lines_gemv(int nb, const double* W, const int* lines,
+                                                    const int* rows, int nrows, const double* rhs,
+                                                    const double* corr, double* out) {
     __shared__ double2 vs[GEMV_COLS];
+    const long long line = lines[blockIdx.z];
+    const double* Wl = W + 2 * line * nb * nb;
+    const double* rl = rhs + 2 * line * nb;
+    const double* cl = corr ? corr + 2 * line * nb : nullptr;
+    double* ol = out + 2 * line * nb;
     const int c0 = blockIdx.x * GEMV_COLS;
     const int ncols = min(GEMV_COLS, nb - c0);
     for (int t = threadIdx.x; t < ncols; t += blockDim.x) {
-        const int b = c0 + t;
-        C2 v = ld2(rhs + 2 * b);
-        if (hprev && pcol[b] >= 0) v = v - ld2(pval + 2 * b) * ld2(hprev + 2 * pcol[b]);
-        if (xnext && ncol[b] >= 0) v = v - ld2(nval + 2 * b) * ld2(xnext + 2 * ncol[b]);
+        C2 v = ld2(rl + 2 * (c0 + t));
+        if (cl) v = v - ld2(cl + 2 * (c0 + t));
         vs[t] = make_double2(v.x, v.y);
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
     for (int q = blockIdx.y * 8 + (threadIdx.x >> 5); q < nrows; q += gridDim.y * 8) {
         const int a = rows ? rows[q] : q;
-        const double2* Wa = reinterpret_cast<const double2*>(W + 2 * ((long long)a * nb + c0));
+        const double2* Wa = reinterpret_cast<const double2*>(Wl + 2 * ((long long)a * nb + c0));
         double2 w[GEMV_COLS / 32];
 #pragma unroll
         for (int e = 0; e < GEMV_COLS / 32; e++) {
@@ -263,9 +247,39 @@ __global__ void __launch_bounds__(256) k_line_gemv(int nb, const double* W, cons
             si += __shfl_xor_sync(0xffffffffu, si, o);
         }
         if (lane == 0) {
-            atomicAdd(out + 2 * a, sr);
-            atomicAdd(out + 2 * a + 1, si);
+            atomicAdd(ol + 2 * a, sr);
+            atomicAdd(ol + 2 * a + 1, si);
         }
+    }
+}
+
+// Couplings between lines, batched: for z < nlines,
+//   dst[lines[z]][rows[i]] += sign * sum_j C[z][i][j] src[nbrs[z]][cols[j]]
+// (C: nlines x R x Q, dense).  A warp per (z, i); lanes walk j.  Every
+// (line, row) pair is written by one warp only.
+__global__ void __launch_bounds__(256) k_couple(int nb, int R, int Q, const double* C, const int* lines,
+                                                const int* nbrs, const int* rows, const int* cols,
+                                                const double* src, double* dst, double sign) {
+    const int z = blockIdx.y;
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (i >= R) return;
+    const double* Ci = C + 2 * ((long long)z * R + i) * Q;
+    const double* s = src + 2 * (long long)nbrs[z] * nb;
+    double sr = 0, si = 0;
+    for (int j = lane; j < Q; j += 32) {
+        const C2 c = ld2(Ci + 2 * j), v = ld2(s + 2 * cols[j]);
+        sr = fma(c.x, v.x, fma(-c.y, v.y, sr));
+        si = fma(c.x, v.y, fma(c.y, v.x, si));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) {
+        double* d = dst + 2 * ((long long)lines[z] * nb + rows[i]);
+        d[0] += sign * sr;
+        d[1] += sign * si;
     }
 }
 
@@ -367,57 +381,41 @@ int FDTD_mode_assemble(const FDTDModeLines* g, int device, void* stream, double 
     return FDTD_OK;
 }
 
-int FDTD_mode_schur(const FDTDModeLines* g, int device, void* stream, int l, double* D, const int* pcol,
-                    const double* pval, const int* ncol, const double* nval) {
+int FDTD_mode_bmul(const FDTDModeLines* g, int device, void* stream, double dir, const double* v,
+                   double* out) {
     Lines G;
-    if (!lines_ok(g, G) || l < 1 || l >= G.NL) return fail(FDTD_ERR_ARG, "FDTD_mode_schur: bad line");
-    MCK(cudaSetDevice(device), "FDTD_mode_schur");
-    const long long blk = (long long)G.nb * G.nb, nthr = blk;
-    const long long off = (long long)l * G.nb;
-    k_schur<<<(unsigned)((nthr + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
-        G.nb, D + 2 * l * blk, D + 2 * (l - 1) * blk, pcol + off, pval + 2 * off, ncol + off - G.nb,
-        nval + 2 * (off - G.nb));
-    MCK(cudaGetLastError(), "FDTD_mode_schur");
+    if (!lines_ok(g, G) || !v || !out) return fail(FDTD_ERR_ARG, "FDTD_mode_bmul: bad arguments");
+    MCK(cudaSetDevice(device), "FDTD_mode_bmul");
+    const long long n = (long long)G.NL * G.nb;
+    k_bmul<<<(unsigned)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096), 256, 0, (cudaStream_t)stream>>>(
+        G, dir, v, out);
+    MCK(cudaGetLastError(), "FDTD_mode_bmul");
     return FDTD_OK;
 }
 
-int FDTD_mode_apply(const FDTDModeLines* g, int device, void* stream, double dir, const double* W,
-                    const int* pcol, const double* pval, const int* ncol, const double* nval, const int* rows,
-                    int nrows, const double* v, int apply_b, double* rhs, double* h, double* x) {
-    Lines G;
-    if (!lines_ok(g, G) || !W || !v || !rhs || !h || !x || (nrows > 0 && !rows))
-        return fail(FDTD_ERR_ARG, "FDTD_mode_apply: bad arguments");
-    MCK(cudaSetDevice(device), "FDTD_mode_apply");
-    cudaStream_t st = (cudaStream_t)stream;
-    const long long n = (long long)G.NL * G.nb;
-    MCK(cudaMemsetAsync(h, 0, sizeof(double) * 2 * n, st), "FDTD_mode_apply");
-    MCK(cudaMemsetAsync(x, 0, sizeof(double) * 2 * n, st), "FDTD_mode_apply");
-    const double* r = v;
-    if (apply_b) {
-        k_bmul<<<(unsigned)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096), 256, 0, st>>>(G, dir, v, rhs);
-        MCK(cudaGetLastError(), "FDTD_mode_apply");
-        r = rhs;
-    }
-    const long long blk = (long long)G.nb * G.nb;
-    const int nr_fwd = nrows > 0 ? nrows : G.nb;
-    const unsigned tiles = (unsigned)((G.nb + GEMV_COLS - 1) / GEMV_COLS);
-    auto grid_for = [tiles](int rows_) { int b = (rows_ + 7) / 8; return dim3(tiles, b < 1 ? 1 : b); };
-    // forward: h_l = W_l (r_l - L_l h_{l-1}) on the rows the next line reads
-    for (int l = 0; l < G.NL; l++) {
-        const long long o = (long long)l * G.nb;
-        k_line_gemv<<<grid_for(nr_fwd), 256, 0, st>>>(
-            G.nb, W + 2 * l * blk, nrows > 0 ? rows : nullptr, nr_fwd, r + 2 * o, pcol + o, pval + 2 * o,
-            l > 0 ? h + 2 * (o - G.nb) : nullptr, ncol + o, nval + 2 * o, nullptr, h + 2 * o);
-    }
-    // backward: x_l = W_l (r_l - L_l h_{l-1} - U_l x_{l+1})
-    for (int l = G.NL - 1; l >= 0; l--) {
-        const long long o = (long long)l * G.nb;
-        k_line_gemv<<<grid_for(G.nb), 256, 0, st>>>(
-            G.nb, W + 2 * l * blk, nullptr, G.nb, r + 2 * o, pcol + o, pval + 2 * o,
-            l > 0 ? h + 2 * (o - G.nb) : nullptr, ncol + o, nval + 2 * o,
-            l < G.NL - 1 ? x + 2 * (o + G.nb) : nullptr, x + 2 * o);
-    }
-    MCK(cudaGetLastError(), "FDTD_mode_apply");
+int FDTD_mode_lines_gemv(int nb, int device, void* stream, const double* W, const int* lines, int nlines,
+                         const int* rows, int nrows, const double* rhs, const double* corr, double* out) {
+    if (nb < 1 || !W || !lines || nlines < 1 || nlines > 65535 || !rhs || !out || (rows && nrows < 1) ||
+        (!rows && nrows != nb))
+        return fail(FDTD_ERR_ARG, "FDTD_mode_lines_gemv: bad arguments");
+    MCK(cudaSetDevice(device), "FDTD_mode_lines_gemv");
+    const unsigned tiles = (unsigned)((nb + GEMV_COLS - 1) / GEMV_COLS);
+    dim3 grid(tiles, (unsigned)((nrows + 7) / 8), (unsigned)nlines);
+    k_lines_gemv<<<grid, 256, 0, (cudaStream_t)stream>>>(nb, W, lines, rows, nrows, rhs, corr, out);
+    MCK(cudaGetLastError(), "FDTD_mode_lines_gemv");
+    return FDTD_OK;
+}
+
+int FDTD_mode_couple(int nb, int device, void* stream, int nlines, int R, int Q, const double* C,
+                     const int* lines, const int* nbrs, const int* rows, const int* cols, const double* src,
+                     double* dst, double sign) {
+    if (nb < 1 || nlines < 1 || nlines > 65535 || R < 1 || Q < 1 || !C || !lines || !nbrs || !rows || !cols ||
+        !src || !dst)
+        return fail(FDTD_ERR_ARG, "FDTD_mode_couple: bad arguments");
+    MCK(cudaSetDevice(device), "FDTD_mode_couple");
+    dim3 grid((unsigned)((R + 7) / 8), (unsigned)nlines);
+    k_couple<<<grid, 256, 0, (cudaStream_t)stream>>>(nb, R, Q, C, lines, nbrs, rows, cols, src, dst, sign);
+    MCK(cudaGetLastError(), "FDTD_mode_couple");
     return FDTD_OK;
 }
 

@@ -212,13 +212,14 @@ libFDTD.FDTD_mode_assemble.argtypes = [c_void_p, c_int, c_void_p, c_double, c_do
                                        c_double, c_double, c_void_p, c_char_p, c_void_p, c_void_p,
                                        c_void_p, c_void_p, c_void_p]
 libFDTD.FDTD_mode_assemble.restype = c_int
-libFDTD.FDTD_mode_schur.argtypes = [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
-                                    c_void_p, c_void_p]
-libFDTD.FDTD_mode_schur.restype = c_int
-libFDTD.FDTD_mode_apply.argtypes = [c_void_p, c_int, c_void_p, c_double, c_void_p, c_void_p, c_void_p,
-                                    c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p,
-                                    c_void_p, c_void_p]
-libFDTD.FDTD_mode_apply.restype = c_int
+libFDTD.FDTD_mode_bmul.argtypes = [c_void_p, c_int, c_void_p, c_double, c_void_p, c_void_p]
+libFDTD.FDTD_mode_bmul.restype = c_int
+libFDTD.FDTD_mode_lines_gemv.argtypes = [c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
+                                         c_int, c_void_p, c_void_p, c_void_p]
+libFDTD.FDTD_mode_lines_gemv.restype = c_int
+libFDTD.FDTD_mode_couple.argtypes = [c_int, c_int, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double]
+libFDTD.FDTD_mode_couple.restype = c_int
 libFDTD.FDTD_mode_source.argtypes = [c_int, c_void_p, c_int, c_int, c_void_p, c_double, c_double,
                                      c_double, c_double, c_double, c_double, c_double, c_void_p,
                                      c_void_p, c_void_p, c_char_p, c_void_p]
@@ -233,7 +234,8 @@ ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_
                  "FDTD_slab_step", "FDTD_slab_halo", "FDTD_slab_sample", "FDTD_slab_probe",
                  "FDTD_slab_capture", "FDTD_slab_finish", "FDTD_structured_values",
                  "FDTD_host_register", "FDTD_host_unregister", "FDTD_mode_last_error",
-                 "FDTD_mode_assemble", "FDTD_mode_schur", "FDTD_mode_apply", "FDTD_mode_source")
+                 "FDTD_mode_assemble", "FDTD_mode_bmul", "FDTD_mode_lines_gemv", "FDTD_mode_couple",
+                 "FDTD_mode_source")
 
 
 class FDTDError(RuntimeError):

@@ -156,57 +156,165 @@ class ModeFullVector:
 
     # --------------------------------------------------------------- solve
     def _factor(self, sigma):
+        """Assemble A - sigma B by lines and factor it by block cyclic
+        reduction: at every level the odd lines of the remaining ones are
+        eliminated (their blocks inverted in one batched call), which leaves
+        dense corrections on the rows of the even lines that couple to them.
+        Every row of a line couples to at most one unknown of the line before
+        (rows P to columns Qp) and one of the line after (rows N to columns
+        Qn), so all couplings stay 2L x 2L blocks Lc (P x Qp) and Uc (N x Qn)."""
         import torch
         g, dev = self._lines, self._dev
         L = self._N if g.sweep_y else self._M
         NL = self._M if g.sweep_y else self._N
         nb = 6 * L
         self._L, self._NL, self._nb = L, NL, nb
-        D = torch.empty((NL, nb, nb), dtype=torch.complex128, device=dev)
+        c128 = torch.complex128
+        D, pcol, pval, ncol, nval = self._assemble(sigma)
+        # the coupling rows and columns, the same on every line that has the neighbour
+        pc, nc = pcol.cpu().numpy(), ncol.cpu().numpy()
+        P = np.flatnonzero(pc[1] >= 0) if NL > 1 else np.zeros(0, dtype=np.int64)
+        Nr = np.flatnonzero(nc[0] >= 0) if NL > 1 else np.zeros(0, dtype=np.int64)
+        Qp, Qn = (pc[1][P], nc[0][Nr]) if NL > 1 else (P, Nr)
+        if NL > 1:
+            ok = (pc[0] < 0).all() and (nc[-1] < 0).all()
+            ok &= all((np.flatnonzero(pc[l] >= 0) == P).all() and (pc[l][P] == Qp).all() for l in range(1, NL))
+            ok &= all((np.flatnonzero(nc[l] >= 0) == Nr).all() and (nc[l][Nr] == Qn).all()
+                      for l in range(NL - 1))
+            ok &= len(np.unique(Qp)) == len(Qp) and len(np.unique(Qn)) == len(Qn)
+            if not ok:
+                raise RuntimeError("line couplings differ from line to line")
+        lt = lambda a: torch.as_tensor(np.asarray(a, dtype=np.int64), device=dev)
+        P_t, N_t, Qp_t, Qn_t = lt(P), lt(Nr), lt(Qp), lt(Qn)
+        nP, nN = len(P), len(Nr)
+        Lc = torch.zeros((NL, nP, nP), dtype=c128, device=dev)
+        Uc = torch.zeros((NL, nN, nN), dtype=c128, device=dev)
+        if NL > 1:
+            ar, an = torch.arange(nP, device=dev), torch.arange(nN, device=dev)
+            Lc[1:, ar, ar] = pval[1:][:, P_t]
+            Uc[:-1, an, an] = nval[:-1][:, N_t]
+
+        def inv_into(lines):
+            W, info = torch.linalg.inv_ex(D[lines])
+            if bool((info != 0).any()):
+                raise RuntimeError("A - n0 B is singular on a line: move n0 off the eigenvalue")
+            D[lines] = W
+
+        levels = []
+        act = list(range(NL))
+        while len(act) > 1:
+            odd, even = act[1::2], act[0::2]
+            e1, o1 = even[1:], odd[:len(even) - 1]          # even[j] with the odd line before it
+            e2, o2 = even[:len(odd)], odd                    # even[j] with the odd line after it
+            has_next = [j for j in range(len(odd)) if j + 1 < len(even)]
+            i32 = lambda a: torch.as_tensor(np.asarray(a, dtype=np.int32), device=dev)
+            odd_n, nxt = [odd[j] for j in has_next], [even[j + 1] for j in has_next]
+            lev = {"odd": lt(odd), "odd32": i32(odd), "e1": lt(e1), "o1": lt(o1), "e2": lt(e2), "o2": lt(o2),
+                   "e1_32": i32(e1), "o1_32": i32(o1), "e2_32": i32(e2), "o2_32": i32(o2),
+                   "Lc_e1": Lc[lt(e1)].clone(), "Uc_e2": Uc[lt(e2)].clone(),
+                   "prev32": i32(even[:len(odd)]), "Lc_odd": Lc[lt(odd)].clone(),
+                   "odd_n32": i32(odd_n), "next32": i32(nxt), "Uc_odd_n": Uc[lt(odd_n)].clone()}
+            inv_into(lev["odd"])
+            newLc = newUc = None
+            if e1:
+                Wq = D[lev["o1"]][:, Qp_t]
+                D.index_put_((lev["e1"][:, None, None], P_t[None, :, None], Qn_t[None, None, :]),
+                             -(Lc[lev["e1"]] @ Wq[:, :, N_t] @ Uc[lev["o1"]]), accumulate=True)
+                newLc = -(Lc[lev["e1"]] @ Wq[:, :, P_t] @ Lc[lev["o1"]])
+            if e2:
+                Wq = D[lev["o2"]][:, Qn_t]
+                D.index_put_((lev["e2"][:, None, None], N_t[None, :, None], Qp_t[None, None, :]),
+                             -(Uc[lev["e2"]] @ Wq[:, :, P_t] @ Lc[lev["o2"]]), accumulate=True)
+                newUc = -(Uc[lev["e2"]] @ Wq[:, :, N_t] @ Uc[lev["o2"]])
+            Lc[even[0]] = 0
+            if newLc is not None:
+                Lc[lev["e1"]] = newLc
+            if newUc is not None:
+                Uc[lev["e2"]] = newUc
+            if len(even) > len(odd):
+                Uc[even[-1]] = 0
+            levels.append(lev)
+            act = even
+        self._top = torch.as_tensor(act, dtype=torch.int32, device=dev)
+        inv_into(lt(act))
+        self._W, self._levels = D, levels
+        self._P, self._Nr, self._Qp, self._Qn = P_t, N_t, Qp_t, Qn_t
+        self._P32, self._N32, self._Qp32, self._Qn32 = (t.to(torch.int32) for t in (P_t, N_t, Qp_t, Qn_t))
+        self._QpQn32 = torch.cat([Qp_t, Qn_t]).unique().to(torch.int32)
+        self._b = torch.empty((NL, nb), dtype=c128, device=dev)
+        self._y = torch.empty((NL, nb), dtype=c128, device=dev)
+        self._xs = torch.empty((NL, nb), dtype=c128, device=dev)
+        self._corr = torch.empty((NL, nb), dtype=c128, device=dev)
+        self.stats_levels = len(levels)
+
+    def _assemble(self, sigma):
+        """Blocks D_l of A - sigma B and the couplings to the neighbouring
+        lines, on the device (FDTD_mode_assemble)."""
+        import torch
+        g, dev, NL, nb = self._lines, self._dev, self._NL, self._nb
+        c128 = torch.complex128
+        D = torch.empty((NL, nb, nb), dtype=c128, device=dev)
         pcol = torch.empty((NL, nb), dtype=torch.int32, device=dev)
         ncol = torch.empty((NL, nb), dtype=torch.int32, device=dev)
-        pval = torch.empty((NL, nb), dtype=torch.complex128, device=dev)
-        nval = torch.empty((NL, nb), dtype=torch.complex128, device=dev)
+        pval = torch.empty((NL, nb), dtype=c128, device=dev)
+        nval = torch.empty((NL, nb), dtype=c128, device=dev)
         planes = (ctypes.c_void_p * 6)(*[p.data_ptr() for p in self._planes])
         stream = torch.cuda.current_stream(dev).cuda_stream
         odx, ody = self.R / self.dx, self.R / self.dy
         _check(libFDTD.FDTD_mode_assemble(ctypes.byref(g), self.device, stream, odx, ody, self._dir,
                                           float(np.real(sigma)), float(np.imag(sigma)), planes,
-                                          self._bc_code(), _ptr(D),
-                                          _ptr(pcol), _ptr(pval), _ptr(ncol), _ptr(nval)),
-               "FDTD_mode_assemble")
-        # every column of line l that a row of line l - 1 reaches is reached once
-        nc = ncol.cpu().numpy()
-        for l in range(NL):
-            c = nc[l][nc[l] >= 0]
-            if len(np.unique(c)) != len(c):
-                raise RuntimeError("line couplings are not one to one")
-        for l in range(NL):
-            if l > 0:
-                _check(libFDTD.FDTD_mode_schur(ctypes.byref(g), self.device, stream, l, _ptr(D), _ptr(pcol),
-                                               _ptr(pval), _ptr(ncol), _ptr(nval)), "FDTD_mode_schur")
-            W, info = torch.linalg.inv_ex(D[l])
-            if int(info) != 0:
-                raise RuntimeError("A - n0 B is singular on line %d: move n0 off the eigenvalue" % l)
-            D[l].copy_(W)
-        rows = torch.unique(pcol[pcol >= 0]).to(torch.int32)
-        self._W, self._pcol, self._pval, self._ncol, self._nval, self._rows = D, pcol, pval, ncol, nval, rows
-        n = NL * nb
-        self._rhs = torch.empty(n, dtype=torch.complex128, device=dev)
-        self._h = torch.empty(n, dtype=torch.complex128, device=dev)
+                                          self._bc_code(), _ptr(D), _ptr(pcol), _ptr(pval), _ptr(ncol),
+                                          _ptr(nval)), "FDTD_mode_assemble")
+        return D, pcol, pval, ncol, nval
 
-    def _apply_direct(self, v, out):
+    def _bmul(self, v, out):
         import torch
         stream = torch.cuda.current_stream(self._dev).cuda_stream
-        _check(libFDTD.FDTD_mode_apply(ctypes.byref(self._lines), self.device, stream, self._dir, _ptr(self._W),
-                                       _ptr(self._pcol), _ptr(self._pval), _ptr(self._ncol), _ptr(self._nval),
-                                       _ptr(self._rows), int(self._rows.numel()), _ptr(v), 1, _ptr(self._rhs),
-                                       _ptr(self._h), _ptr(out)), "FDTD_mode_apply")
+        _check(libFDTD.FDTD_mode_bmul(ctypes.byref(self._lines), self.device, stream, self._dir, _ptr(v),
+                                      _ptr(out)), "FDTD_mode_bmul")
+
+    def _gemv(self, lines32, rows32, rhs, corr, out):
+        import torch
+        stream = torch.cuda.current_stream(self._dev).cuda_stream
+        nrows = int(rows32.numel()) if rows32 is not None else self._nb
+        _check(libFDTD.FDTD_mode_lines_gemv(self._nb, self.device, stream, _ptr(self._W), _ptr(lines32),
+                                            int(lines32.numel()), _ptr(rows32) if rows32 is not None else None,
+                                            nrows, _ptr(rhs), _ptr(corr) if corr is not None else None,
+                                            _ptr(out)), "FDTD_mode_lines_gemv")
+
+    def _couple(self, lines32, nbrs32, C, rows32, cols32, src, dst, sign):
+        import torch
+        stream = torch.cuda.current_stream(self._dev).cuda_stream
+        _check(libFDTD.FDTD_mode_couple(self._nb, self.device, stream, int(lines32.numel()), int(rows32.numel()),
+                                        int(cols32.numel()), _ptr(C), _ptr(lines32), _ptr(nbrs32), _ptr(rows32),
+                                        _ptr(cols32), _ptr(src), _ptr(dst), float(sign)), "FDTD_mode_couple")
+
+    def _apply_direct(self, v, out):
+        """out = (A - n0 B)^-1 B v: reduction over the levels, the top line,
+        back-substitution over the levels."""
+        b, y, x, corr = self._b, self._y, self._xs, self._corr
+        self._bmul(v, b)
+        y.zero_()
+        x.zero_()
+        corr.zero_()
+        for lev in self._levels:
+            self._gemv(lev["odd32"], self._QpQn32, b, None, y)
+            if lev["e1_32"].numel():
+                self._couple(lev["e1_32"], lev["o1_32"], lev["Lc_e1"], self._P32, self._Qp32, y, b, -1.0)
+            if lev["e2_32"].numel():
+                self._couple(lev["e2_32"], lev["o2_32"], lev["Uc_e2"], self._N32, self._Qn32, y, b, -1.0)
+        self._gemv(self._top, None, b, None, x)
+        for lev in reversed(self._levels):
+            self._couple(lev["odd32"], lev["prev32"], lev["Lc_odd"], self._P32, self._Qp32, x, corr, 1.0)
+            if lev["odd_n32"].numel():
+                self._couple(lev["odd_n32"], lev["next32"], lev["Uc_odd_n"], self._N32, self._Qn32, x, corr, 1.0)
+            self._gemv(lev["odd32"], None, b, corr, x)
+        out.copy_(x.view(-1))
         return out
 
     def _capture(self):
-        """One application of (A - n0 B)^-1 B (2 NL sweep launches) as a CUDA
-        graph on fixed buffers, replayed by :meth:`_apply`."""
+        """One application of (A - n0 B)^-1 B as a CUDA graph on fixed
+        buffers, replayed by :meth:`_apply`."""
         import torch
         n = self._NL * self._nb
         self._vin = torch.zeros(n, dtype=torch.complex128, device=self._dev)
@@ -267,7 +375,7 @@ class ModeFullVector:
         self._neff = np.zeros(k, dtype=np.complex128)
         self._neff[:len(theta)] = sigma + 1.0 / np.asarray(theta)
         self.stats = {"factor_s": t1 - t0, "iterate_s": t2 - t1, "applications": napply,
-                      "lines": self._NL, "block": self._nb}
+                      "lines": self._NL, "block": self._nb, "levels": self.stats_levels}
 
     # ----------------------------------------------------------- the fields
     def _raw(self, i, component):

@@ -345,9 +345,9 @@ int FDTD_structured_values(int device, void *stream, const double *zs, int nzs,
  * holds nb = 6 L unknowns (Ex Ey Ez Hx Hy Hz blocks of L), NL lines in all;
  * vectors are complex128 in line order ((l * 6 + c) * L + p).  All pointers
  * are device memory; complex values are interleaved (re, im) doubles.  The
- * dense inverses of the Schur complements are the caller's (a device LU):
- * after FDTD_mode_assemble, for l = 0, 1, ...: FDTD_mode_schur(l) (l >= 1),
- * then replace block l of D by its inverse. */
+ * caller factors the block-tridiagonal A - n0 B (block cyclic reduction with
+ * a device LU for the dense inverses) and applies its inverse with
+ * FDTD_mode_lines_gemv over the lines of each reduction level. */
 typedef struct FDTDModeLines {
     int M, N;
     int sweep_y;
@@ -367,19 +367,25 @@ int FDTD_mode_assemble(const FDTDModeLines *g, int device, void *stream, double 
                        double dir, double sigma_re, double sigma_im, const double *const *planes,
                        const char *bc, double *D, int *pcol, double *pval, int *ncol, double *nval);
 
-/* Schur complement of line l >= 1 in place: D_l -= L_l D_{l-1} U_{l-1}, with
- * D_{l-1} already replaced by its inverse. */
-int FDTD_mode_schur(const FDTDModeLines *g, int device, void *stream, int l, double *D,
-                    const int *pcol, const double *pval, const int *ncol, const double *nval);
+/* out = B v (line order; B of emopt/modes.py:1361-1585, dir: +1 or -1). */
+int FDTD_mode_bmul(const FDTDModeLines *g, int device, void *stream, double dir, const double *v,
+                   double *out);
 
-/* x = (A - sigma B)^-1 (B v) (apply_b) or (A - sigma B)^-1 v, with W the
- * inverted blocks: a forward and a backward sweep over the lines.  rows[nrows]:
- * the local columns that rows of the next line reference (every pcol value);
- * rhs, h: NL x nb scratch; x: NL x nb. */
-int FDTD_mode_apply(const FDTDModeLines *g, int device, void *stream, double dir, const double *W,
-                    const int *pcol, const double *pval, const int *ncol, const double *nval,
-                    const int *rows, int nrows, const double *v, int apply_b, double *rhs, double *h,
-                    double *x);
+/* Batched over lines: for l = lines[0..nlines-1],
+ *   out_l[a] += sum_b W_l[a][b] (rhs_l[b] - corr_l[b])
+ * for the rows a in rows[0..nrows-1] (rows null: all nb rows, nrows = nb);
+ * W: NL x nb x nb blocks, rhs/corr/out: NL x nb (corr may be null; out is
+ * accumulated into, so zero it first). */
+int FDTD_mode_lines_gemv(int nb, int device, void *stream, const double *W, const int *lines,
+                         int nlines, const int *rows, int nrows, const double *rhs,
+                         const double *corr, double *out);
+
+/* Couplings between lines, batched over z < nlines:
+ *   dst[lines[z]][rows[i]] += sign * sum_j C[z][i][j] src[nbrs[z]][cols[j]],
+ * C: nlines x R x Q dense complex128, src/dst: NL x nb (line order). */
+int FDTD_mode_couple(int nb, int device, void *stream, int nlines, int R, int Q, const double *C,
+                     const int *lines, const int *nbrs, const int *rows, const int *cols,
+                     const double *src, double *dst, double sign);
 
 /* Current sources of a mode (ModeFullVector.get_source, emopt/modes.py:2144-
  * 2296) from its six raw field planes (fields: [6][M][N], solver order):

@@ -87,3 +87,77 @@ def test_product_interpolation_matches_oracle(ndir, shape, bc):
         assert m.get_field(0, c).shape == shape
         want = O.get_field_interp(vec, c, M, N, ndir, bc)
         np.testing.assert_allclose(m.get_field_interp(0, c, squeeze=True), want, rtol=0, atol=1e-15)
+
+
+def _line_order(M, N, sweep_y):
+    L, NL = (N, M) if sweep_y else (M, N)
+    perm = np.empty(NL * 6 * L, dtype=np.int64)
+    for l in range(NL):
+        for c in range(6):
+            for p in range(L):
+                y, x = (l, p) if sweep_y else (p, l)
+                perm[(l * 6 + c) * L + p] = c * M * N + y * N + x
+    return perm, L, NL
+
+
+@pytest.mark.parametrize("M,N,sweep,bc,back", [
+    (6, 7, "y", ("0", "0"), False), (6, 7, "x", ("0", "0"), False), (9, 5, "y", ("E", "H"), True),
+    (9, 5, "x", ("H", "E"), False), (2, 3, "y", ("0", "0"), False), (1, 4, "y", ("0", "0"), False),
+    (13, 4, "y", ("0", "0"), False), (4, 16, "x", ("E", "0"), True)])
+def test_product_cyclic_reduction_solves_the_system(M, N, sweep, bc, back):
+    """The product's block cyclic reduction (factor and the application of
+    (A - n0 B)^-1 B), run on the CPU with its three device calls (assembly,
+    B v, the batched line GEMV) emulated exactly from the oracle's A and B,
+    equals a dense solve of the same system."""
+    torch = pytest.importorskip("torch")
+    from emopt_b200.grid import ConstantMaterial3D
+    from emopt_b200.misc import DomainCoordinates
+    from emopt_b200.modes import ModeFullVector
+    sigma = 3.1
+    A, B = O.build_system(_layered(M, N, 4), M, N, 0.05, 0.06, WL, bc=bc, backwards=back)
+    dom = DomainCoordinates.from_indices(0, N, 0, M, 0, 1, 0.05, 0.06, 0.05)
+    m = ModeFullVector(WL, ConstantMaterial3D(2.0), ConstantMaterial3D(1.0), dom, device=0, sweep=sweep)
+    m._dev = torch.device("cpu")
+    perm, L, NL = _line_order(M, N, bool(m._lines.sweep_y))
+    nb = 6 * L
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm))
+    T = (A - sigma * B).toarray()[np.ix_(perm, perm)]
+    Bl = B.toarray()[np.ix_(perm, perm)]
+    Acoo = A.tocoo()
+
+    def assemble(sig):
+        D = torch.as_tensor(np.stack([T[l * nb:(l + 1) * nb, l * nb:(l + 1) * nb] for l in range(NL)]))
+        pcol, ncol = -torch.ones(NL, nb, dtype=torch.int32), -torch.ones(NL, nb, dtype=torch.int32)
+        pval, nval = torch.zeros(NL, nb, dtype=torch.complex128), torch.zeros(NL, nb, dtype=torch.complex128)
+        for i, j, v in zip(inv[Acoo.row], inv[Acoo.col], Acoo.data):
+            li, lj = i // nb, j // nb
+            if lj == li - 1:
+                pcol[li, i % nb], pval[li, i % nb] = int(j % nb), v
+            elif lj == li + 1:
+                ncol[li, i % nb], nval[li, i % nb] = int(j % nb), v
+        return D, pcol, pval, ncol, nval
+
+    def gemv(lines32, rows32, rhs, corr, out):
+        for l in lines32.tolist():
+            r = m._W[l] @ (rhs[l] - (corr[l] if corr is not None else 0))
+            if rows32 is None:
+                out[l] += r
+            else:
+                out[l, rows32.long()] += r[rows32.long()]
+
+    def couple(lines32, nbrs32, C, rows32, cols32, src, dst, sign):
+        for z, (l, n) in enumerate(zip(lines32.tolist(), nbrs32.tolist())):
+            dst[l, rows32.long()] += sign * (C[z] @ src[n, cols32.long()])
+
+    m._couple = couple
+    m._assemble = assemble
+    m._bmul = lambda v, out: out.view(-1).copy_(torch.as_tensor(Bl) @ v)
+    m._gemv = gemv
+    m._factor(sigma)
+    rng = np.random.default_rng(0)
+    v = torch.as_tensor(rng.standard_normal(NL * nb) + 1j * rng.standard_normal(NL * nb))
+    out = torch.empty_like(v)
+    m._apply_direct(v, out)
+    want = np.linalg.solve(T, Bl @ v.numpy())
+    assert np.linalg.norm(out.numpy() - want) < 1e-12 * np.linalg.norm(want)
