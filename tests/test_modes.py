@@ -161,3 +161,28 @@ def test_product_cyclic_reduction_solves_the_system(M, N, sweep, bc, back):
     m._apply_direct(v, out)
     want = np.linalg.solve(T, Bl @ v.numpy())
     assert np.linalg.norm(out.numpy() - want) < 1e-12 * np.linalg.norm(want)
+
+
+@pytest.mark.parametrize("k,m", [(1, 16), (4, 24), (6, 14)])
+def test_krylov_schur_finds_largest_modulus_eigenpairs(k, m):
+    """The product's Krylov-Schur iteration (run on the CPU with a dense
+    operator) returns the k eigenvalues of largest modulus of a non-normal
+    matrix with a slowly decaying spectrum -- restarts included -- and their
+    eigenvectors."""
+    torch = pytest.importorskip("torch")
+    from emopt_b200.modes import _krylov_schur
+    rng = np.random.default_rng(k)
+    n = 300
+    lam = (0.97 ** np.arange(n)) * np.exp(1j * rng.uniform(0, 2 * np.pi, n))
+    X = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    A = X @ np.diag(lam) @ np.linalg.inv(X)
+    At = torch.as_tensor(A)
+    apply = lambda v, out: out.copy_(At @ v)
+    v0 = torch.as_tensor(rng.standard_normal(n) + 0j)
+    theta, V, nconv, napply = _krylov_schur(apply, n, k, m, 1e-12, 200, v0, torch.device("cpu"))
+    assert nconv == k and napply > m            # it had to restart
+    want = lam[np.argsort(-np.abs(lam))[:k]]
+    np.testing.assert_allclose(np.sort_complex(theta), np.sort_complex(want), rtol=1e-9)
+    for q in range(k):
+        x = V[q].numpy()
+        assert np.linalg.norm(A @ x - theta[q] * x) < 1e-8 * np.linalg.norm(x) * abs(theta[q])
