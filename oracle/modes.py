@@ -21,11 +21,12 @@ gives; any phase is an eigenvector).
 
 Parity unpinned against the reference itself: petsc4py and slepc4py are not
 in this image, so ``ModeFullVector`` cannot run here.  The assembly is pinned
-by a known answer instead: for a uniform medium in the PEC box every finite
+by a known answer instead: for a uniform medium in the box every nonzero
 eigenvalue satisfies the discrete dispersion relation of the compressed Yee
-grid, n^2 = eps mu - (2/dx sin(p pi/2N))^2 - (2/dy sin(q pi/2M))^2
-(tests/test_modes.py), and the shift-invert solve by a dense eigen-solve of
-the same pencil.
+grid, n^2 = eps mu - (2R/dx sin(p pi/2N))^2 - (2R/dy sin(q pi/2M))^2, with
+the half-shifted wavenumbers sin((p + 1/2) pi/2N) for the second parity
+along an axis with the 'E' symmetry letter (tests/test_modes.py); the
+shift-invert solve is pinned by a dense eigen-solve of the same pencil.
 """
 from __future__ import annotations
 
@@ -373,10 +374,17 @@ def get_source(vec, neff, M, N, ndir, bc, wavelength, dx, dy, dz, eps_plane, mu_
     return Jx, Jy, Jz, Mx, My, Mz
 
 
-def discrete_box_spectrum(eps, mu, M, N, dx, dy, wavelength):
-    """n^2 of every mode of a uniform medium in the PEC box of the compressed
-    Yee grid (p = 0..N-1, q = 0..M-1, not both 0)."""
+def discrete_box_spectrum(eps, mu, M, N, dx, dy, wavelength, bc=("0", "0")):
+    """n^2 allowed for a uniform medium in the box of the compressed Yee grid:
+    eps mu - kx^2 - ky^2 with kx = 2R/dx sin(p pi/2N), ky = 2R/dy sin(q pi/2M)
+    (p = 0..N-1, q = 0..M-1); where an axis has the 'E' symmetry letter, the
+    modes of the other parity take the half-shifted wavenumbers
+    sin((p + 1/2) pi/2N) along it, so the spectrum is the union of both
+    families.  Flattened."""
     R = wavelength / (2 * np.pi)
-    kx = 2 * R / dx * np.sin(np.arange(N) * np.pi / (2 * N))
-    ky = 2 * R / dy * np.sin(np.arange(M) * np.pi / (2 * M))
-    return eps * mu - kx[None, :] ** 2 - ky[:, None] ** 2
+
+    def k(n, d, half):
+        return 2 * R / d * np.sin((np.arange(n) + (0.5 if half else 0.0)) * np.pi / (2 * n))
+
+    fam = [(k(N, dx, False), k(M, dy, False)), (k(N, dx, bc[0] == "E"), k(M, dy, bc[1] == "E"))]
+    return np.concatenate([(eps * mu - kx[None, :] ** 2 - ky[:, None] ** 2).ravel() for kx, ky in fam])
