@@ -4,9 +4,9 @@ FDTD_BOUNDS_CHECK) runs the parity cases of the production kernels.
 In that build every index the vector pair and the serving kernel compute is
 checked against its array before the access; a lane out of range records the
 site and skips, and the solve, slab and serving calls then return an error.
-The selected tests (fp64 golden boxes, ragged row tails, converging step
-counts, fp32 error bounds, z slabs at fixed step counts, serving) therefore
-pass only if no index of theirs leaves its array.  They run in a child
+The selected tests (fp64 golden boxes, every boundary combination, ragged
+row tails, converging step counts, fp32 error bounds, z slabs at fixed step
+counts, serving) therefore pass only if no index of theirs leaves its array.  They run in a child
 process, which loads the checked library through EMOPT_B200_LIB.
 """
 import os
@@ -19,7 +19,8 @@ from helpers import ROOT
 
 pytestmark = pytest.mark.gpu
 
-SELECT = "(test_gpu_parity and vector and not vector16) or test_fixed_steps or test_gpu_serving"
+SELECT = ("(test_gpu_parity and vector and not vector16) or every_bc or test_fixed_steps "
+          "or test_gpu_serving")
 
 
 def test_parity_cases_pass_with_index_checks():

@@ -136,6 +136,25 @@ def test_solve_cw_fp64_matches_golden(name, kernel):
     assert rel_l2(F, g["fields"]) < 1e-11
 
 
+BC_ALL = [a + b + c for a in "0EH" for b in "0EH" for c in "0EH"]
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("bc", BC_ALL)
+def test_solve_cw_fp64_every_bc_matches_oracle(bc, cplx):
+    """Every boundary combination {0, E, H}^3, lossless and lossy, through the
+    default stepping kernels: the same tiny blocks on which the oracle equals
+    the reference core bit for bit (tests/test_oracle.py), solved on the GPU
+    in fp64 and compared with the oracle run here."""
+    k = BC_ALL.index(bc)
+    p = P.random_box(100 + 2 * k + cplx, shape=(5, 6, 7), w_pml=(2, 1, 1, 2, 2, 1), bc=bc,
+                     complex_eps=cplx, mu_random=bool(k % 2), edge_source=True, fixed_steps=50)
+    ref = oracle_for(p, oracle_lib()).solve(fixed_steps=p.fixed_steps)
+    F, info, _ = solve_gpu(p, "fp64", "auto")
+    assert info["steps"] == ref["steps"]
+    assert rel_l2(F, np.stack(ref["fields"])) < 1e-11
+
+
 @pytest.mark.parametrize("kernel", ["vector", "scalar"])
 @pytest.mark.parametrize("name", list(TAIL_KW))
 def test_row_tail_matches_golden(name, kernel):
