@@ -319,6 +319,9 @@ class ModeFullVector:
         n = self._NL * self._nb
         self._vin = torch.zeros(n, dtype=torch.complex128, device=self._dev)
         self._xout = torch.empty(n, dtype=torch.complex128, device=self._dev)
+        self._graph = None
+        if self._dev.type != "cuda":      # host emulation of the device calls (tests)
+            return
         self._apply_direct(self._vin, self._xout)          # outside the capture first
         torch.cuda.synchronize(self._dev)
         g = torch.cuda.CUDAGraph()
@@ -327,10 +330,17 @@ class ModeFullVector:
         self._graph = g
 
     def _apply(self, v, out):
+        if self._graph is None:
+            return self._apply_direct(v, out)
         self._vin.copy_(v)
         self._graph.replay()
         out.copy_(self._xout)
         return out
+
+    def _sync(self):
+        import torch
+        if self._dev.type == "cuda":
+            torch.cuda.synchronize(self._dev)
 
     def _to_solver_order(self, X):
         """[k][NL*nb] line order -> [k][6][M][N]."""
@@ -351,7 +361,7 @@ class ModeFullVector:
         sigma = complex(self.n0)
         self._factor(sigma)
         self._capture()
-        torch.cuda.synchronize(self._dev)
+        self._sync()
         t1 = time.perf_counter()
         k = self.neigs
         m = ncv or max(3 * k, k + 20)
@@ -360,7 +370,7 @@ class ModeFullVector:
         rng = np.random.default_rng(seed)
         v0 = torch.as_tensor(rng.standard_normal(n) + 1j * rng.standard_normal(n), device=self._dev)
         theta, X, nconv, napply = _krylov_schur(self._apply, n, k, m, tol, maxit, v0, self._dev)
-        torch.cuda.synchronize(self._dev)
+        self._sync()
         t2 = time.perf_counter()
         if nconv < k:
             warning_message("%d eigenmodes were requested, however only %d eigenmodes were found."

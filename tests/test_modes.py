@@ -102,33 +102,20 @@ def _line_order(M, N, sweep_y):
     return perm, L, NL
 
 
-@pytest.mark.parametrize("M,N,sweep,bc,back", [
-    (6, 7, "y", ("0", "0"), False), (6, 7, "x", ("0", "0"), False), (9, 5, "y", ("E", "H"), True),
-    (9, 5, "x", ("H", "E"), False), (2, 3, "y", ("0", "0"), False), (1, 4, "y", ("0", "0"), False),
-    (13, 4, "y", ("0", "0"), False), (4, 16, "x", ("E", "0"), True)])
-def test_product_cyclic_reduction_solves_the_system(M, N, sweep, bc, back):
-    """The product's block cyclic reduction (factor and the application of
-    (A - n0 B)^-1 B), run on the CPU with its three device calls (assembly,
-    B v, the batched line GEMV) emulated exactly from the oracle's A and B,
-    equals a dense solve of the same system."""
-    torch = pytest.importorskip("torch")
-    from emopt_b200.grid import ConstantMaterial3D
-    from emopt_b200.misc import DomainCoordinates
-    from emopt_b200.modes import ModeFullVector
-    sigma = 3.1
-    A, B = O.build_system(_layered(M, N, 4), M, N, 0.05, 0.06, WL, bc=bc, backwards=back)
-    dom = DomainCoordinates.from_indices(0, N, 0, M, 0, 1, 0.05, 0.06, 0.05)
-    m = ModeFullVector(WL, ConstantMaterial3D(2.0), ConstantMaterial3D(1.0), dom, device=0, sweep=sweep)
+def _emulate_device(m, A, B, M, N):
+    """Replace the product's device calls (assembly, B v, batched line GEMV,
+    couplings) by exact host computations from the oracle's A and B."""
+    import torch
     m._dev = torch.device("cpu")
     perm, L, NL = _line_order(M, N, bool(m._lines.sweep_y))
     nb = 6 * L
     inv = np.empty_like(perm)
     inv[perm] = np.arange(len(perm))
-    T = (A - sigma * B).toarray()[np.ix_(perm, perm)]
-    Bl = B.toarray()[np.ix_(perm, perm)]
+    Al, Bl = A.toarray()[np.ix_(perm, perm)], B.toarray()[np.ix_(perm, perm)]
     Acoo = A.tocoo()
 
     def assemble(sig):
+        T = Al - sig * Bl
         D = torch.as_tensor(np.stack([T[l * nb:(l + 1) * nb, l * nb:(l + 1) * nb] for l in range(NL)]))
         pcol, ncol = -torch.ones(NL, nb, dtype=torch.int32), -torch.ones(NL, nb, dtype=torch.int32)
         pval, nval = torch.zeros(NL, nb, dtype=torch.complex128), torch.zeros(NL, nb, dtype=torch.complex128)
@@ -152,17 +139,67 @@ def test_product_cyclic_reduction_solves_the_system(M, N, sweep, bc, back):
         for z, (l, n) in enumerate(zip(lines32.tolist(), nbrs32.tolist())):
             dst[l, rows32.long()] += sign * (C[z] @ src[n, cols32.long()])
 
-    m._couple = couple
-    m._assemble = assemble
+    m._assemble, m._gemv, m._couple = assemble, gemv, couple
     m._bmul = lambda v, out: out.view(-1).copy_(torch.as_tensor(Bl) @ v)
-    m._gemv = gemv
+    return Al, Bl, perm
+
+
+@pytest.mark.parametrize("M,N,sweep,bc,back", [
+    (6, 7, "y", ("0", "0"), False), (6, 7, "x", ("0", "0"), False), (9, 5, "y", ("E", "H"), True),
+    (9, 5, "x", ("H", "E"), False), (2, 3, "y", ("0", "0"), False), (1, 4, "y", ("0", "0"), False),
+    (13, 4, "y", ("0", "0"), False), (4, 16, "x", ("E", "0"), True)])
+def test_product_cyclic_reduction_solves_the_system(M, N, sweep, bc, back):
+    """The product's block cyclic reduction (factor and the application of
+    (A - n0 B)^-1 B), run on the CPU with its device calls emulated exactly
+    from the oracle's A and B, equals a dense solve of the same system."""
+    torch = pytest.importorskip("torch")
+    from emopt_b200.grid import ConstantMaterial3D
+    from emopt_b200.misc import DomainCoordinates
+    from emopt_b200.modes import ModeFullVector
+    sigma = 3.1
+    A, B = O.build_system(_layered(M, N, 4), M, N, 0.05, 0.06, WL, bc=bc, backwards=back)
+    dom = DomainCoordinates.from_indices(0, N, 0, M, 0, 1, 0.05, 0.06, 0.05)
+    m = ModeFullVector(WL, ConstantMaterial3D(2.0), ConstantMaterial3D(1.0), dom, device=0, sweep=sweep)
+    Al, Bl, _ = _emulate_device(m, A, B, M, N)
     m._factor(sigma)
+    n = Al.shape[0]
     rng = np.random.default_rng(0)
-    v = torch.as_tensor(rng.standard_normal(NL * nb) + 1j * rng.standard_normal(NL * nb))
+    v = torch.as_tensor(rng.standard_normal(n) + 1j * rng.standard_normal(n))
     out = torch.empty_like(v)
     m._apply_direct(v, out)
-    want = np.linalg.solve(T, Bl @ v.numpy())
+    want = np.linalg.solve(Al - sigma * Bl, Bl @ v.numpy())
     assert np.linalg.norm(out.numpy() - want) < 1e-12 * np.linalg.norm(want)
+
+
+@pytest.mark.parametrize("sweep,bc,back", [("y", ("0", "0"), False), ("x", ("E", "H"), True)])
+def test_product_solve_matches_oracle_host_emulated(sweep, bc, back):
+    """ModeFullVector.solve end to end on the CPU (factor, Krylov-Schur,
+    ordering, normalisation, field access, interpolation) with the device
+    calls emulated from the oracle's A and B: the oracle's modes."""
+    torch = pytest.importorskip("torch")
+    from emopt_b200.grid import ConstantMaterial3D
+    from emopt_b200.misc import DomainCoordinates
+    from emopt_b200.modes import ModeFullVector
+    M, N, n0, k = 8, 11, 3.3, 3
+    A, B = O.build_system(_layered(M, N, 1), M, N, 0.05, 0.06, WL, bc=bc, backwards=back)
+    dom = DomainCoordinates.from_indices(0, N, 0, M, 0, 1, 0.05, 0.06, 0.05)
+    m = ModeFullVector(WL, ConstantMaterial3D(2.0), ConstantMaterial3D(1.0), dom, n0=n0, neigs=k,
+                       backwards=back, device=0, sweep=sweep)
+    m.bc = list(bc)
+    _emulate_device(m, A, B, M, N)
+    m._planes = []                                   # sampled planes are not used by the emulation
+    m.solve()
+    neff, V = O.solve(A, B, n0, k)
+    np.testing.assert_allclose(m.neff, neff, rtol=1e-10)
+    for q in range(k):
+        got = np.concatenate([m.get_field(q, c, permute=False, squeeze=True).ravel() for c in O.COMPONENTS])
+        assert np.linalg.norm(got) == pytest.approx(1.0, abs=1e-12)
+        c = np.vdot(got, V[q])
+        c /= abs(c)
+        assert np.linalg.norm(got * c - V[q]) < 1e-8
+        for comp in O.COMPONENTS:
+            want = O.get_field_interp(V[q], comp, M, N, "z", bc)
+            assert np.linalg.norm(m.get_field_interp(q, comp, squeeze=True) * c - want) < 1e-8
 
 
 @pytest.mark.parametrize("k,m", [(1, 16), (4, 24), (6, 14)])
