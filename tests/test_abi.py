@@ -103,3 +103,23 @@ def test_argument_errors_are_reported():
     assert "precision" in ct.last_error(h)[1]
     assert ct.libFDTD.FDTD_set_kernel(h, 8) == ct.FDTD_ERR_ARG
     ct.libFDTD.FDTD_delete(h)
+
+
+def test_mode_entry_points_reject_bad_arguments():
+    """The mode-solver entry points validate their arguments before any CUDA
+    call and report FDTD_ERR_ARG with a message."""
+    from emopt_b200 import fdtd_ctypes as ct
+    lib = ct.libFDTD
+    g = ct.ModeLines(0, 5, 1)
+    assert lib.FDTD_mode_assemble(ctypes.byref(g), 0, None, 1.0, 1.0, 1.0, 3.0, 0.0, None, b"00",
+                                  None, None, None, None, None) == ct.FDTD_ERR_ARG
+    assert b"FDTD_mode_assemble" in lib.FDTD_mode_last_error()
+    assert lib.FDTD_mode_bmul(None, 0, None, 1.0, None, None) == ct.FDTD_ERR_ARG
+    dummy = ctypes.c_void_p(16)
+    assert lib.FDTD_mode_lines_gemv(6, 0, None, dummy, dummy, 0, None, 6, dummy, None, dummy) == ct.FDTD_ERR_ARG
+    assert lib.FDTD_mode_lines_gemv(6, 0, None, dummy, dummy, 1, None, 5, dummy, None, dummy) == ct.FDTD_ERR_ARG
+    assert b"lines_gemv" in lib.FDTD_mode_last_error()
+    assert lib.FDTD_mode_couple(6, 0, None, 1, 0, 2, dummy, dummy, dummy, dummy, dummy, dummy, dummy,
+                                1.0) == ct.FDTD_ERR_ARG
+    assert lib.FDTD_mode_source(0, None, 0, 3, dummy, 1.0, 0.0, 1.0, 0.0, 1.0, 1.0, 1.0, dummy, dummy,
+                                dummy, b"00", dummy) == ct.FDTD_ERR_ARG
