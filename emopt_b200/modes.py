@@ -177,10 +177,9 @@ class ModeFullVector:
         Nr = np.flatnonzero(nc[0] >= 0) if NL > 1 else np.zeros(0, dtype=np.int64)
         Qp, Qn = (pc[1][P], nc[0][Nr]) if NL > 1 else (P, Nr)
         if NL > 1:
-            ok = (pc[0] < 0).all() and (nc[-1] < 0).all()
-            ok &= all((np.flatnonzero(pc[l] >= 0) == P).all() and (pc[l][P] == Qp).all() for l in range(1, NL))
-            ok &= all((np.flatnonzero(nc[l] >= 0) == Nr).all() and (nc[l][Nr] == Qn).all()
-                      for l in range(NL - 1))
+            ok = bool((pc[0] < 0).all() and (nc[-1] < 0).all())
+            ok &= bool(((pc[1:] >= 0) == (pc[1] >= 0)).all() and (pc[1:, P] == Qp).all())
+            ok &= bool(((nc[:-1] >= 0) == (nc[0] >= 0)).all() and (nc[:-1, Nr] == Qn).all())
             ok &= len(np.unique(Qp)) == len(Qp) and len(np.unique(Qn)) == len(Qn)
             if not ok:
                 raise RuntimeError("line couplings differ from line to line")
