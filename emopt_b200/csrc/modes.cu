@@ -366,6 +366,7 @@ int FDTD_mode_assemble(const FDTDModeLines* g, int device, void* stream, double 
     Lines G;
     if (!lines_ok(g, G) || !planes || !bc || !D || !pcol || !pval || !ncol || !nval)
         return fail(FDTD_ERR_ARG, "FDTD_mode_assemble: bad arguments");
+    if (G.NL > 65535) return fail(FDTD_ERR_ARG, "FDTD_mode_assemble: more than 65535 lines");
     MCK(cudaSetDevice(device), "FDTD_mode_assemble");
     Planes P;
     for (int q = 0; q < 6; q++) {
