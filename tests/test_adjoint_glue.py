@@ -116,3 +116,35 @@ def test_reference_calc_gradient_formula():
     g = R.calc_gradient(x, y, eps0, steps, step)
     exact = [-2 * np.real(sum(np.sum(y[c] * 1j * dd[c] * x[c]) for c in range(3))) for dd in dirs]
     np.testing.assert_allclose(g, exact, rtol=1e-9)
+
+
+@pytest.mark.parametrize("bc", ["000", "EH0", "0HE"])
+def test_source_power_matches_reference_formula(bc):
+    """The torch source power over the six planes one cell inside the CPML
+    (emopt/fdtd.py:1555-1667; planes on symmetric min faces left out), on
+    random fields, against the same sums over the oracle's interpolation."""
+    from types import SimpleNamespace
+    Nz, Ny, Nx = SHAPE
+    dx, dy, dz = D
+    rng = np.random.default_rng(11)
+    full = _rand_fields(rng)
+    sim = SimpleNamespace(dx=dx, dy=dy, dz=dz, _w_pml=(2 * dx, 3 * dx, 2 * dy, 0.0, 2 * dz, 2 * dz),
+                          X=(Nx - 1) * dx, Y=(Ny - 1) * dy, Z=(Nz - 1) * dz, bc=bc)
+    planes = A.source_power_planes(sim)
+    assert len(planes) == 6 - sum(c in "EH" for c in bc)
+    grown = [A.grow_domain(dom, SHAPE, D) for dom, _, _ in planes]
+    raws = [torch.as_tensor(np.stack([f[g.i1:g.i2, g.j1:g.j2, g.k1:g.k2] for f in full])) for g in grown]
+    got = float(A.source_power(raws, planes, grown, sim))
+    want = 0.0
+    dA = {0: dy * dz, 1: dx * dz, 2: dx * dy}
+    for dom, axis, sign in planes:
+        rb = R.Box(dom.k1, dom.k2, dom.j1, dom.j2, dom.i1, dom.i2)
+        f = {comp: R.interp(full[c], comp, rb, bc, D) for c, comp in enumerate(A.COMPONENTS)}
+        if axis == 0:
+            s = f["Ey"] * np.conj(f["Hz"]) - f["Ez"] * np.conj(f["Hy"])
+        elif axis == 1:
+            s = -(f["Ex"] * np.conj(f["Hz"]) - f["Ez"] * np.conj(f["Hx"]))
+        else:
+            s = f["Ex"] * np.conj(f["Hy"]) - f["Ey"] * np.conj(f["Hx"])
+        want += sign * 0.5 * dA[axis] * np.sum(s.real)
+    assert got == pytest.approx(want, rel=1e-12)
