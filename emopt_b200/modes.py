@@ -510,18 +510,27 @@ class ModeFullVector:
         return Jx, Jy, Jz, Mx, My, Mz
 
 
-def _krylov_schur(apply, n, k, m, tol, maxit, v0, dev):
+def _krylov_schur(apply, n, k, m, tol, maxit, v0, dev, check_every=4):
     """Krylov-Schur iteration for the k eigenvalues of largest modulus of the
-    operator ``apply`` (n x n, device vectors), m-dimensional subspace.
-    Returns (theta[k'], vectors[k'][n], k' converged, applications)."""
+    operator ``apply`` (n x n, device vectors), m-dimensional subspace; the
+    Ritz values are tested every ``check_every`` new vectors, so a solve stops
+    as soon as the wanted pairs have converged.  Returns (theta[k'],
+    vectors[k'][n], k' converged, applications)."""
     import torch
     V = torch.empty((m + 1, n), dtype=torch.complex128, device=dev)
     H = np.zeros((m + 1, m), dtype=np.complex128)
     V[0] = v0 / torch.linalg.vector_norm(v0)
     w = torch.empty(n, dtype=torch.complex128, device=dev)
-    p, napply = 0, 0
-    theta = S = order = None
+    p, napply, mc = 0, 0, 0
+
+    def ritz(size):
+        theta, S = np.linalg.eig(H[:size, :size])
+        order = np.argsort(-np.abs(theta))
+        res = np.abs(H[size, size - 1] * S[size - 1, :])
+        return theta, S, order, res
+
     for _ in range(maxit):
+        done = False
         for j in range(p, m):
             apply(V[j], w)
             napply += 1
@@ -534,20 +543,23 @@ def _krylov_schur(apply, n, k, m, tol, maxit, v0, dev):
             beta = float(torch.linalg.vector_norm(w))
             H[:j + 1, j] = h.cpu().numpy()
             H[j + 1, j] = beta
-            if beta == 0.0:
-                m = j + 1
+            mc = j + 1
+            if beta == 0.0:                        # an invariant subspace: the Ritz pairs are exact
+                done = True
                 break
             V[j + 1] = w / beta
-        Hm = H[:m, :m]
-        theta, S = np.linalg.eig(Hm)
-        order = np.argsort(-np.abs(theta))
-        res = np.abs(H[m, m - 1] * S[m - 1, :])
-        done = [res[q] <= tol * abs(theta[q]) for q in order[:k]]
-        if all(done) or H[m, m - 1] == 0:
+            if mc == m or (mc >= k + 2 and (mc - p) % check_every == 0):
+                theta, S, order, res = ritz(mc)
+                if all(res[q] <= tol * abs(theta[q]) for q in order[:k]):
+                    done = True
+                    break
+        if done:
             break
+        # restart: keep the Schur vectors of the wanted part and some more
+        theta, S, order, res = ritz(m)
         keep = min(m - 1, max(k + (m - k) // 2, k + 1))
         thr = np.abs(theta[order[keep - 1]])
-        T, Z, sdim = sla.schur(Hm, output="complex", sort=lambda z: abs(z) >= thr * (1 - 1e-12))
+        T, Z, sdim = sla.schur(H[:m, :m], output="complex", sort=lambda z: abs(z) >= thr * (1 - 1e-12))
         p = int(min(max(sdim, k), m - 1))
         Zt = torch.as_tensor(np.ascontiguousarray(Z[:, :p].T), device=dev)
         V[:p] = Zt @ V[:m]
@@ -556,8 +568,8 @@ def _krylov_schur(apply, n, k, m, tol, maxit, v0, dev):
         Hn[:p, :p] = T[:p, :p]
         Hn[p, :p] = H[m, m - 1] * Z[m - 1, :p]
         H = Hn
-    res = np.abs(H[m, m - 1] * S[m - 1, :])
+    theta, S, order, res = ritz(mc)
     good = [q for q in order[:k] if res[q] <= max(tol, 1e-8) * abs(theta[q])]
     Sk = torch.as_tensor(np.ascontiguousarray(S[:, good].T), device=dev)
-    X = Sk @ V[:m]
+    X = Sk @ V[:mc]
     return theta[good], X, len(good), napply
