@@ -716,6 +716,31 @@ class FDTD(MaxwellSolver):
         grad_mu = sm * (lam / size - del_mu * gh)
         return np.concatenate([np.ravel(grad_eps), np.ravel(grad_mu)])
 
+    def calc_ydAx_autograd(self, domain, update_mu, eps_autograd, mu_autograd):
+        """Pseudo figure of merit for reverse-mode autodiff of the material
+        arrays (``emopt/experimental/fdtd.py:160-223``):
+        ``2 sum Im(eps . E . E_adj)`` over the domain, minus
+        ``2 sum Im(mu . H . H_adj)`` when ``update_mu``.  ``eps_autograd`` /
+        ``mu_autograd``: three torch tensors each (the staggered x, y, z
+        arrays on the domain), on any device; the fields follow them there, so
+        the gradient with respect to them is the adjoint overlap."""
+        import torch
+
+        def pair(c, like):
+            f = torch.as_tensor(self.get_field(c, domain)).to(like.device)
+            a = torch.as_tensor(self.get_adjoint_field(c, domain)).to(like.device)
+            return f, a
+
+        loss = 0
+        for c, e in zip(("Ex", "Ey", "Ez"), eps_autograd):
+            f, a = pair(c, e)
+            loss = loss + e * f * a
+        if update_mu:
+            for c, m in zip(("Hx", "Hy", "Hz"), mu_autograd):
+                f, a = pair(c, m)
+                loss = loss - m * f * a
+        return 2 * loss.imag.sum()
+
     def calc_ydAx(self, Adiag0):
         """y^T dA x with dA = i (eps - eps0) for E and -i (mu - mu0) for H
         (``emopt/fdtd.py:1694-1717``)."""

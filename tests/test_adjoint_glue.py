@@ -148,3 +148,35 @@ def test_source_power_matches_reference_formula(bc):
             s = f["Ex"] * np.conj(f["Hy"]) - f["Ey"] * np.conj(f["Hx"])
         want += sign * 0.5 * dA[axis] * np.sum(s.real)
     assert got == pytest.approx(want, rel=1e-12)
+
+
+@pytest.mark.parametrize("update_mu", [False, True])
+def test_calc_ydAx_autograd_pseudo_loss(update_mu):
+    """FDTD.calc_ydAx_autograd (emopt/experimental/fdtd.py:160-223): its value
+    is 2 sum Im(eps E E_adj) (- 2 sum Im(mu H H_adj)), and autograd gives the
+    adjoint overlap 2 Im(E E_adj) as the gradient of a real permittivity."""
+    from types import SimpleNamespace
+
+    from emopt_b200.fdtd import FDTD
+    rng = np.random.default_rng(5)
+    fwd = dict(zip(A.COMPONENTS, _rand_fields(rng)))
+    adj = dict(zip(A.COMPONENTS, _rand_fields(rng)))
+    dom = DomainCoordinates.from_indices(2, 9, 1, 7, 3, 6, *D)
+    take = lambda a: a[dom.i1:dom.i2, dom.j1:dom.j2, dom.k1:dom.k2]
+    fake = SimpleNamespace(get_field=lambda c, d: take(fwd[c]), get_adjoint_field=lambda c, d: take(adj[c]))
+    shape = take(fwd["Ex"]).shape
+    eps = [torch.as_tensor(rng.uniform(1, 12, shape)).requires_grad_(True) for _ in range(3)]
+    mu = [torch.as_tensor(rng.uniform(1, 2, shape)).requires_grad_(True) for _ in range(3)]
+    loss = FDTD.calc_ydAx_autograd(fake, dom, update_mu, eps, mu)
+    want = sum(2 * np.sum(np.imag(e.detach().numpy() * take(fwd[c]) * take(adj[c])))
+               for c, e in zip(("Ex", "Ey", "Ez"), eps))
+    if update_mu:
+        want -= sum(2 * np.sum(np.imag(m.detach().numpy() * take(fwd[c]) * take(adj[c])))
+                    for c, m in zip(("Hx", "Hy", "Hz"), mu))
+    assert float(loss) == pytest.approx(want, rel=1e-12)
+    loss.backward()
+    for c, e in zip(("Ex", "Ey", "Ez"), eps):
+        np.testing.assert_allclose(e.grad.numpy(), 2 * np.imag(take(fwd[c]) * take(adj[c])), rtol=1e-12)
+    if update_mu:
+        np.testing.assert_allclose(mu[0].grad.numpy(), -2 * np.imag(take(fwd["Hx"]) * take(adj["Hx"])),
+                                   rtol=1e-12)
