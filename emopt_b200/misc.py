@@ -82,5 +82,16 @@ class DomainCoordinates:
         d.set_region(k1, k2, j1, j2, i1, i2, dx, dy, dz)
         return d
 
+    def grow(self, x1, x2, y1, y2, z1, z2):
+        """Grow by the given numbers of cells towards -x, +x, -y, +y, -z, +z
+        (negative values shrink; not checked), ``emopt/misc.py`` grow."""
+        self.set_region(self.k1 - x1, self.k2 + x2, self.j1 - y1, self.j2 + y2, self.i1 - z1,
+                        self.i2 + z2, self._dx, self._dy, self._dz)
+
+    def copy(self):
+        """A new domain with the same index ranges and spacings."""
+        return DomainCoordinates.from_indices(self.k1, self.k2, self.j1, self.j2, self.i1, self.i2,
+                                              self._dx, self._dy, self._dz)
+
     def get_bounding_box(self):
         return [self._x[0], self._x[-1], self._y[0], self._y[-1], self._z[0], self._z[-1]]

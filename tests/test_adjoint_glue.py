@@ -180,3 +180,53 @@ def test_calc_ydAx_autograd_pseudo_loss(update_mu):
     if update_mu:
         np.testing.assert_allclose(mu[0].grad.numpy(), -2 * np.imag(take(fwd["Hx"]) * take(adj["Hx"])),
                                    rtol=1e-12)
+
+
+@pytest.mark.parametrize("normal", [(1, 0, 0), (0, -1, 0), (0, 0, 1)])
+def test_fomutils_mode_match_matches_restatement(normal):
+    """emopt_b200.fomutils.ModeMatch (the reference's numpy interface) against
+    the oracle's restatement: forward match and every derivative; the
+    backward match is the forward match of the mode with H reversed."""
+    from emopt_b200.fomutils import ModeMatch
+    rng = np.random.default_rng(sum(normal) + 7)
+    shape = (1, 6, 9)
+    r = lambda: rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    mode = {c: r() for c in A.COMPONENTS}
+    fields = {c: r() for c in A.COMPONENTS}
+    mm = ModeMatch(normal, 0.05, 0.04, **{c + "m": mode[c] for c in A.COMPONENTS})
+    mm.compute(**fields)
+    F, dF = R.mode_match(fields, mode, normal, 0.05, 0.04)
+    assert mm.get_mode_match_forward(1.0) == pytest.approx(F, rel=1e-12)
+    for c in A.COMPONENTS:
+        np.testing.assert_allclose(getattr(mm, "get_dFd" + c)(), dF[c], rtol=1e-12, atol=1e-15)
+    back = {c: (-fields[c] if c[0] == "H" else fields[c]) for c in A.COMPONENTS}
+    mm2 = ModeMatch(normal, 0.05, 0.04, **{c + "m": mode[c] for c in A.COMPONENTS})
+    mm2.compute(**back)
+    assert mm2.get_mode_match_back(2.0) == pytest.approx(mm.get_mode_match_forward(2.0), rel=1e-12)
+
+
+@pytest.mark.parametrize("bc", ["000", "HH0", "EE0", "HE0"])
+@pytest.mark.parametrize("box", [(0, 5, 0, 6, 2, 4), (3, 8, 2, 7, 1, 6), (4, 5, 0, 12, 0, 9)])
+def test_fomutils_interpolated_dFdx_matches_restatement(box, bc):
+    from types import SimpleNamespace
+
+    from emopt_b200.fomutils import interpolated_dFdx_3D
+    rng = np.random.default_rng(13)
+    dom = DomainCoordinates.from_indices(*box, *D)
+    dF = [rng.standard_normal(dom.shape) + 1j * rng.standard_normal(dom.shape) for _ in range(6)]
+    g, *got = interpolated_dFdx_3D(SimpleNamespace(bc=bc), dom, *dF)
+    rg, want = R.interpolated_dFdx(R.Box(*box), dict(zip(A.COMPONENTS, dF)), bc)
+    assert (g.k1, g.k2, g.j1, g.j2, g.i1, g.i2) == (rg.k1, rg.k2, rg.j1, rg.j2, rg.i1, rg.i2)
+    assert (dom.k1, dom.j1, dom.i2) == (box[0], box[2], box[5])          # the input is not changed
+    for a, c in zip(got, A.COMPONENTS):
+        assert a.shape == g.shape
+        np.testing.assert_allclose(a, want[c], rtol=0, atol=1e-15)
+
+
+def test_domain_grow_and_copy():
+    d = DomainCoordinates.from_indices(2, 5, 3, 7, 1, 4, 0.1, 0.2, 0.3)
+    e = d.copy()
+    e.grow(1, 2, 0, 1, 1, 0)
+    assert (d.k1, d.k2, d.j1, d.j2, d.i1, d.i2) == (2, 5, 3, 7, 1, 4)
+    assert (e.k1, e.k2, e.j1, e.j2, e.i1, e.i2) == (1, 7, 3, 8, 0, 4)
+    assert e.shape == (4, 5, 6) and np.allclose(e.x, 0.1 * np.arange(1, 7))
