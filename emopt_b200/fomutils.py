@@ -137,8 +137,8 @@ def interpolated_dFdx_3D(sim, domain, dFdExi, dFdEyi, dFdEzi, dFdHxi, dFdHyi, dF
                     a[1 + dz:1 + dz + Nz, 1, 1:1 + Nx] -= v[:, 0, :]
         if c in ("Ey", "Hx", "Hz") and domain.j1 == 0 and bc[1] in "EH":
             sgn = 1.0 if bc[1] == "H" else -1.0
-            for dz, _, dx in taps:
-                if _ == 0:
+            for dz, dy, dx in taps:
+                if dy == 0:
                     a[1 + dz:1 + dz + Nz, 1, 1 + dx:1 + dx + Nx] += sgn * v[:, 0, :]
         if c == "Ez":
             a[1:-1, 1:-1, 1:-1] = dF[c]
@@ -146,3 +146,53 @@ def interpolated_dFdx_3D(sim, domain, dFdExi, dFdEyi, dFdEzi, dFdHxi, dFdHyi, dF
     grown = domain.copy()
     grown.grow(1, 0, 1, 0, 0, 1)
     return (grown, *out)
+
+
+# Derivative of the plane flux s (E x H*) . e_axis with respect to each
+# interpolated component, before the factor 0.25 dA and the outward sign:
+# (component, sign, conjugated partner).
+_DFLUX = {
+    0: [("Ey", 1.0, "Hz"), ("Ez", -1.0, "Hy"), ("Hy", -1.0, "Ez"), ("Hz", 1.0, "Ey")],
+    1: [("Ex", -1.0, "Hz"), ("Ez", 1.0, "Hx"), ("Hx", 1.0, "Ez"), ("Hz", -1.0, "Ex")],
+    2: [("Ex", 1.0, "Hy"), ("Ey", -1.0, "Hx"), ("Hx", -1.0, "Ey"), ("Hy", 1.0, "Ex")],
+}
+
+
+def power_norm_dFdx_3D(sim, f, domain, dfdEx, dfdEy, dfdEz, dfdHx, dfdHy, dfdHz):
+    """Adjoint sources of F = f / Psrc (emopt/fomutils.py:1654-1920): the
+    derivative of f (with respect to interpolated fields on ``domain``)
+    divided by the source power, plus -f / Psrc^2 times the derivative of the
+    source power through each of the six planes one cell inside the CPML
+    (planes on symmetric min faces left out), every block mapped to the
+    staggered fields by :func:`interpolated_dFdx_3D`.  Returns
+    [sources, domains].  As in the reference, a face without CPML puts its
+    plane at the domain edge (X, not X - dx as the source power itself)."""
+    Psrc = sim.source_power
+    srcs, doms = [], []
+    g = interpolated_dFdx_3D(sim, domain, *(np.asarray(a) / Psrc for a in
+                                            (dfdEx, dfdEy, dfdEz, dfdHx, dfdHy, dfdHz)))
+    srcs.append(g[1:])
+    doms.append(g[0])
+    w = sim.w_pml
+    d = (sim.dx, sim.dy, sim.dz)
+    L = (sim.X, sim.Y, sim.Z)
+    lo = [w[2 * a] + d[a] if w[2 * a] > 0 else 0.0 for a in range(3)]
+    hi = [L[a] - w[2 * a + 1] - d[a] if w[2 * a + 1] > 0 else L[a] for a in range(3)]
+    from .misc import DomainCoordinates
+    for axis in range(3):
+        for side, pos in ((-1.0, lo[axis]), (1.0, hi[axis])):
+            if side < 0 and sim.bc[axis] in ("E", "H"):
+                continue
+            b = [[lo[0], hi[0]], [lo[1], hi[1]], [lo[2], hi[2]]]
+            b[axis] = [pos, pos]
+            plane = DomainCoordinates(b[0][0], b[0][1], b[1][0], b[1][1], b[2][0], b[2][1], *d)
+            dA = np.prod([d[q] for q in range(3) if q != axis])
+            need = {p for _, _, p in _DFLUX[axis]}
+            F = {c: sim.get_field_interp(c, domain=plane) for c in sorted(need)}
+            dP = {c: np.zeros(plane.shape, dtype=np.complex128) for c in _C}
+            for c, sgn, partner in _DFLUX[axis]:
+                dP[c] = -1 * f * (side * sgn * 0.25 * dA * np.conj(F[partner])) / Psrc ** 2
+            g = interpolated_dFdx_3D(sim, plane, *(dP[c] for c in _C))
+            srcs.append(g[1:])
+            doms.append(g[0])
+    return [srcs, doms]

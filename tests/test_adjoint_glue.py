@@ -230,3 +230,80 @@ def test_domain_grow_and_copy():
     assert (d.k1, d.k2, d.j1, d.j2, d.i1, d.i2) == (2, 5, 3, 7, 1, 4)
     assert (e.k1, e.k2, e.j1, e.j2, e.i1, e.i2) == (1, 7, 3, 8, 0, 4)
     assert e.shape == (4, 5, 6) and np.allclose(e.x, 0.1 * np.arange(1, 7))
+
+
+def _fake_sim(full, bc, w=2):
+    """A stand-in for FDTD: fields interpolated by the oracle, the source
+    power summed over the planes of the reference's get_source_power."""
+    from types import SimpleNamespace
+    Nz, Ny, Nx = SHAPE
+    dx, dy, dz = D
+    sim = SimpleNamespace(dx=dx, dy=dy, dz=dz, X=(Nx - 1) * dx, Y=(Ny - 1) * dy, Z=(Nz - 1) * dz, bc=bc,
+                          w_pml=[w * dx, w * dx, w * dy, w * dy, w * dz, w * dz])
+    sim._w_pml = sim.w_pml
+    sim.get_field_interp = lambda c, domain=None, squeeze=False: R.interp(
+        full[A.COMPONENTS.index(c)], c, R.Box(domain.k1, domain.k2, domain.j1, domain.j2, domain.i1, domain.i2),
+        bc, D)
+    P = 0.0
+    dA = {0: dy * dz, 1: dx * dz, 2: dx * dy}
+    for dom, axis, sign in A.source_power_planes(sim):
+        f = {c: sim.get_field_interp(c, dom) for c in A.COMPONENTS}
+        cj = np.conj
+        s = {0: f["Ey"] * cj(f["Hz"]) - f["Ez"] * cj(f["Hy"]),
+             1: -(f["Ex"] * cj(f["Hz"]) - f["Ez"] * cj(f["Hx"])),
+             2: f["Ex"] * cj(f["Hy"]) - f["Ey"] * cj(f["Hx"])}[axis]
+        P += sign * 0.5 * dA[axis] * np.sum(s.real)
+    sim.source_power = P
+    return sim
+
+
+@pytest.mark.parametrize("bc", ["000", "0H0", "0E0", "H0E"])
+def test_power_norm_dFdx_3D_matches_finite_differences(bc):
+    """power_norm_dFdx_3D + interpolated_dFdx_3D (the reference's adjoint
+    sources of F = f / Psrc, f a mode match) against central differences of F
+    in the raw staggered fields: for a real F, dF/d(Re z) = 2 Re(dF/dz) and
+    dF/d(Im z) = -2 Im(dF/dz)."""
+    from emopt_b200.fomutils import ModeMatch, power_norm_dFdx_3D
+    rng = np.random.default_rng(21)
+    full = _rand_fields(rng)
+    mon = DomainCoordinates.from_indices(9, 10, 3, 9, 3, 7, *D)
+    mode = {c + "m": rng.standard_normal(mon.shape) + 1j * rng.standard_normal(mon.shape) for c in A.COMPONENTS}
+
+    def F_of(fields):
+        sim = _fake_sim(fields, bc)
+        mm = ModeMatch((1, 0, 0), D[1], D[2], **mode)
+        mm.compute(**{c: sim.get_field_interp(c, mon) for c in A.COMPONENTS})
+        return mm, sim, mm.mode_match_fwd.real / sim.source_power
+
+    mm, sim, F0 = F_of(full)
+    f = mm.mode_match_fwd.real
+    srcs, doms = power_norm_dFdx_3D(sim, f, mon, mm.get_dFdEx(), mm.get_dFdEy(), mm.get_dFdEz(),
+                                    mm.get_dFdHx(), mm.get_dFdHy(), mm.get_dFdHz())
+    assert len(srcs) == 1 + 6 - sum(c in "EH" for c in bc)
+    D_full = [np.zeros(SHAPE, dtype=np.complex128) for _ in range(6)]
+    for arrays, g in zip(srcs, doms):
+        for c in range(6):
+            sl = (slice(g.i1, g.i2), slice(g.j1, g.j2), slice(g.k1, g.k2))
+            blk = np.asarray(arrays[c])
+            assert blk.shape == g.shape
+            # blocks may reach one cell past the grid (grown domain): clip
+            i2, j2, k2 = min(g.i2, SHAPE[0]), min(g.j2, SHAPE[1]), min(g.k2, SHAPE[2])
+            D_full[c][g.i1:i2, g.j1:j2, g.k1:k2] += blk[:i2 - g.i1, :j2 - g.j1, :k2 - g.k1]
+    picks = []
+    for c in range(6):
+        nz = np.argwhere(np.abs(D_full[c]) > 0)
+        for q in rng.choice(len(nz), size=min(6, len(nz)), replace=False):
+            picks.append((c, tuple(nz[q])))
+        # and anywhere (mostly where the sources are zero: F must not move)
+        for _ in range(3):
+            picks.append((c, tuple(int(rng.integers(0, n)) for n in SHAPE)))
+    h = 1e-6
+    for c, pos in picks:
+        for direction in (1.0, 1j):
+            up = [a.copy() for a in full]
+            dn = [a.copy() for a in full]
+            up[c][pos] += h * direction
+            dn[c][pos] -= h * direction
+            fd = (F_of(up)[2] - F_of(dn)[2]) / (2 * h)
+            want = 2 * np.real(D_full[c][pos] * direction)
+            assert fd == pytest.approx(want, rel=1e-5, abs=1e-9 * abs(F0)), (c, pos, direction)
