@@ -307,3 +307,158 @@ def test_power_norm_dFdx_3D_matches_finite_differences(bc):
             fd = (F_of(up)[2] - F_of(dn)[2]) / (2 * h)
             want = 2 * np.real(D_full[c][pos] * direction)
             assert fd == pytest.approx(want, rel=1e-5, abs=1e-9 * abs(F0)), (c, pos, direction)
+
+
+def test_adjoint_method_calc_gradient_is_the_reference_formula():
+    """AdjointMethod.calc_gradient over FDTD.calc_ydAx: one perturbation per
+    parameter, -2 Re(y^T dA x / step), parameters and materials restored."""
+    import types
+
+    from emopt_b200.adjoint_method import AdjointMethod
+    from emopt_b200.fdtd import FDTD
+    rng = np.random.default_rng(4)
+    n = int(np.prod(SHAPE))
+    sim = types.SimpleNamespace(ndims=3, X=1.0, Y=1.0, Z=1.0, dx=0.05, updates=[])
+    for c in A.COMPONENTS:
+        for kind in ("fwd", "adj"):
+            setattr(sim, "_%s_%s_t0" % (c, kind), rng.standard_normal(n) + 1j * rng.standard_normal(n))
+    base = [rng.uniform(2, 12, n) + 0j for _ in range(3)]
+    masks = [rng.uniform(0, 1, (3, n)) for _ in range(4)]
+    sim._mu_x = sim._mu_y = sim._mu_z = np.ones(n, dtype=np.complex128)
+    sim.update = lambda box=None: sim.updates.append(box)
+    sim.calc_ydAx = types.MethodType(FDTD.calc_ydAx, sim)
+    sim.get_A_diag = types.MethodType(FDTD.get_A_diag, sim)
+
+    class AM(AdjointMethod):
+        def update_system(self, params):
+            for a, name in enumerate(("_eps_x", "_eps_y", "_eps_z")):
+                setattr(sim, name, base[a] + sum(p * m[a] for p, m in zip(params, masks)))
+
+        def calc_fom(self, sim, params):
+            return 0.0
+
+        def calc_dFdx(self, sim, params):
+            return [[], []]
+
+        def calc_grad_p(self, sim, params):
+            return 0.0
+
+    params = np.array([0.3, -0.2, 0.5, 0.1])
+    am = AM(sim, step=1e-6)
+    am.update_system(params)
+    eps0 = [sim._eps_x.copy(), sim._eps_y.copy(), sim._eps_z.copy()]
+    g = am.calc_gradient(sim, params)
+    assert np.array_equal(params, [0.3, -0.2, 0.5, 0.1])
+    assert all(np.array_equal(e, getattr(sim, nm)) for e, nm in zip(eps0, ("_eps_x", "_eps_y", "_eps_z")))
+    assert len(sim.updates) == 2 * len(params) and sim.updates[0] == (0, 1.0, 0, 1.0, 0, 1.0)
+    x = [getattr(sim, "_%s_fwd_t0" % c) for c in ("Ex", "Ey", "Ez")]
+    y = [getattr(sim, "_%s_adj_t0" % c) for c in ("Ex", "Ey", "Ez")]
+    steps = []
+    for i in range(len(params)):
+        p = params.copy()
+        p[i] += 1e-6
+        steps.append([base[a] + sum(q * m[a] for q, m in zip(p, masks)) for a in range(3)])
+    want = R.calc_gradient(x, y, eps0, steps, 1e-6)
+    np.testing.assert_allclose(g, want, rtol=1e-6)
+    # linear in the parameters: the derivative is -2 Re(i y . mask . x)
+    exact = [-2 * np.real(1j * sum(np.sum(y[a] * m[a] * x[a]) for a in range(3))) for m in masks]
+    np.testing.assert_allclose(g, exact, rtol=1e-6)
+
+
+def test_adjoint_method_gradient_and_check_gradient_flow():
+    """gradient(): forward solve, adjoint sources, adjoint solve, then
+    calc_gradient + calc_grad_p; check_gradient compares with finite
+    differences of fom and reports the total relative error."""
+    from types import SimpleNamespace
+
+    from emopt_b200.adjoint_method import AdjointMethod
+    calls = []
+    sim = SimpleNamespace(ndims=3, X=1.0, Y=1.0, Z=1.0, dx=0.05)
+    sim.update = lambda box=None: calls.append("update")
+    sim.solve_forward = lambda: calls.append("forward")
+    sim.solve_adjoint = lambda: calls.append("adjoint")
+    sim.set_adjoint_sources = lambda src: calls.append(("sources", src))
+    state = {}
+
+    class AM(AdjointMethod):
+        def update_system(self, params):
+            state["p"] = np.array(params, dtype=float)
+
+        def calc_fom(self, sim, params):
+            return float(np.sum(np.sin(state["p"])) + 0.5 * state["p"][0] ** 2)
+
+        def calc_dFdx(self, sim, params):
+            return [["dF"], ["dom"]]
+
+        def calc_gradient(self, sim, params):
+            return np.cos(np.asarray(params, dtype=float))
+
+        def calc_grad_p(self, sim, params):
+            g = np.zeros(len(params))
+            g[0] = params[0]
+            return g
+
+    am = AM(sim)
+    p = np.array([0.2, 1.1, -0.7])
+    g = am.gradient(p)
+    np.testing.assert_allclose(g, np.cos(p) + np.array([0.2, 0, 0]))
+    assert calls[:4] == ["update", "forward", ("sources", [["dF"], ["dom"]]), "adjoint"]
+    err = am.check_gradient(p.copy(), plot=False, verbose=False, fd_step=1e-7)
+    assert err < 1e-5
+
+    class Wrong(AM):
+        def calc_grad_p(self, sim, params):
+            return np.zeros(len(params))
+
+    with pytest.warns(UserWarning, match="over 1%"):
+        err2, gfd, gam = Wrong(sim).check_gradient(p.copy(), indices=[0, 2], plot=False, verbose=False,
+                                                  return_gradients=True, fd_step=1e-7)
+    assert err2 > 0.01 and len(gfd) == 2
+
+
+def test_adjoint_method_pnf3d_fom_and_sources():
+    """AdjointMethodPNF3D: F = f / Psrc + penalty and the adjoint sources of
+    power_norm_dFdx_3D for each fom domain."""
+    from emopt_b200.adjoint_method import AdjointMethodPNF3D
+    from emopt_b200.fomutils import ModeMatch, power_norm_dFdx_3D
+    rng = np.random.default_rng(8)
+    full = _rand_fields(rng)
+    sim = _fake_sim(full, "000")
+    mon = DomainCoordinates.from_indices(9, 10, 3, 9, 3, 7, *D)
+    mode = {c + "m": rng.standard_normal(mon.shape) + 1j * rng.standard_normal(mon.shape) for c in A.COMPONENTS}
+
+    class AM(AdjointMethodPNF3D):
+        def update_system(self, params):
+            pass
+
+        def _mm(self, sim):
+            mm = ModeMatch((1, 0, 0), D[1], D[2], **mode)
+            mm.compute(**{c: sim.get_field_interp(c, mon) for c in A.COMPONENTS})
+            return mm
+
+        def calc_f(self, sim, params):
+            return self._mm(sim).mode_match_fwd.real
+
+        def calc_dfdx(self, sim, params):
+            mm = self._mm(sim)
+            return [[mm.get_dFdEx(), mm.get_dFdEy(), mm.get_dFdEz(), mm.get_dFdHx(), mm.get_dFdHy(),
+                     mm.get_dFdHz()]]
+
+        def get_fom_domains(self):
+            return [mon]
+
+        def calc_penalty(self, sim, params):
+            return 0.25
+
+        def calc_grad_p(self, sim, params):
+            return 0.0
+
+    am = AM(sim)
+    f = am.calc_f(sim, [])
+    assert am.calc_fom(sim, []) == pytest.approx(f / sim.source_power + 0.25)
+    srcs, doms = am.calc_dFdx(sim, [])
+    want_s, want_d = power_norm_dFdx_3D(sim, f, mon, *am.calc_dfdx(sim, [])[0])
+    assert len(srcs) == len(want_s) == 7
+    for a, b in zip(srcs, want_s):
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
