@@ -215,3 +215,65 @@ class AdjointMethodPNF3D(AdjointMethod):
             a_src = fomutils.power_norm_dFdx_3D(sim, f, domain, *dfdxs[i])
             sources = [sources[0] + a_src[0], sources[1] + a_src[1]]
         return sources
+
+
+class AdjointMethodMO(AdjointMethod):
+    """Several adjoint methods combined into one figure of merit
+    (emopt/adjoint_method.py:723-929): subclasses define
+    ``calc_total_fom(foms)`` and ``calc_total_gradient(foms, grads)``."""
+
+    def __init__(self, ams, step=1e-6):
+        self._ams = ams
+        self._foms_current = np.zeros(len(ams))
+        self._step = step
+        self.prev_params = []
+        self._grad_f_time = 0.0
+
+    @property
+    def adjoint_methods(self):
+        return self._ams
+
+    @adjoint_methods.setter
+    def adjoint_methods(self, new_ams):
+        self._ams = new_ams
+
+    def update_system(self, params):
+        for am in self._ams:
+            am.update_system(params)
+
+    def calc_fom(self, sim, params):
+        return self.calc_total_fom(self._foms_current)
+
+    def calc_dFdx(self, sim, params):
+        return None
+
+    def calc_grad_p(self, sim, params):
+        return None
+
+    @abstractmethod
+    def calc_total_fom(self, foms):
+        """The combined figure of merit from the individual ones."""
+
+    @abstractmethod
+    def calc_total_gradient(self, foms, grads):
+        """The combined gradient from the individual figures and gradients."""
+
+    def fom(self, params):
+        foms = [am.fom(params) for am in self._ams]
+        self._foms_current = foms
+        return self.calc_total_fom(foms)
+
+    def gradient(self, params):
+        foms, grads = [], []
+        for am in self._ams:
+            grads.append(am.gradient(params))
+            foms.append(am.calc_fom(am.sim, params))
+        return self.calc_total_gradient(foms, grads)
+
+    def check_gradient(self, params, indices=[], plot=True, verbose=True, return_gradients=False,
+                       fd_step=1e-10):
+        self.sim = self._ams[0].sim
+        for am in self._ams:
+            am.update_system(params)
+            am.sim.update()
+        return super().check_gradient(params, indices, plot, verbose, return_gradients, fd_step)

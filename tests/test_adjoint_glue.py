@@ -462,3 +462,48 @@ def test_adjoint_method_pnf3d_fom_and_sources():
     for a, b in zip(srcs, want_s):
         for x, y in zip(a, b):
             np.testing.assert_array_equal(x, y)
+
+
+def test_adjoint_method_mo_combines_objectives():
+    """AdjointMethodMO: the combined figure of merit and gradient of several
+    adjoint methods, checked against finite differences."""
+    from types import SimpleNamespace
+
+    from emopt_b200.adjoint_method import AdjointMethod, AdjointMethodMO
+
+    def make(scale):
+        sim = SimpleNamespace(ndims=3, X=1.0, Y=1.0, Z=1.0, dx=0.05)
+        sim.update = lambda box=None: None
+        sim.solve_forward = sim.solve_adjoint = lambda: None
+        sim.set_adjoint_sources = lambda src: None
+        st = {}
+
+        class AM(AdjointMethod):
+            def update_system(self, params):
+                st["p"] = np.array(params, dtype=float)
+
+            def calc_fom(self, sim, params):
+                return float(scale * np.sum(st["p"] ** 2))
+
+            def calc_dFdx(self, sim, params):
+                return [[], []]
+
+            def calc_gradient(self, sim, params):
+                return 2 * scale * np.asarray(params, dtype=float)
+
+            def calc_grad_p(self, sim, params):
+                return 0.0
+        return AM(sim)
+
+    class MO(AdjointMethodMO):
+        def calc_total_fom(self, foms):
+            return foms[0] * foms[1]
+
+        def calc_total_gradient(self, foms, grads):
+            return foms[1] * grads[0] + foms[0] * grads[1]
+
+    mo = MO([make(1.0), make(3.0)])
+    p = np.array([0.4, -0.3])
+    assert mo.fom(p) == pytest.approx(np.sum(p ** 2) * 3 * np.sum(p ** 2))
+    np.testing.assert_allclose(mo.gradient(p), 2 * 6 * np.sum(p ** 2) * p)
+    assert mo.check_gradient(p.copy(), plot=False, verbose=False, fd_step=1e-7) < 1e-5
