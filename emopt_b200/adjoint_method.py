@@ -11,6 +11,8 @@ this package's FDTD solver, so that optimisation scripts written as
 * ``AdjointMethodPNF3D`` (emopt/adjoint_method.py:1329-1486): figures of
   merit normalised by the source power, F = f / Psrc + penalty, with the
   adjoint sources of ``fomutils.power_norm_dFdx_3D``.
+* ``AdjointMethodMO`` (emopt/adjoint_method.py:723-929): several adjoint
+  methods combined through ``calc_total_fom`` / ``calc_total_gradient``.
 
 The solves and the overlap products run on the GPU (``FDTD.solve_forward`` /
 ``solve_adjoint`` through ``FDTD_solve_cw``); one process owns the whole grid,
