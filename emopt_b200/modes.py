@@ -215,15 +215,17 @@ class ModeFullVector:
                    "odd_n32": i32(odd_n), "next32": i32(nxt), "Uc_odd_n": Uc[lt(odd_n)].clone()}
             inv_into(lev["odd"])
             newLc = newUc = None
+            # the corrections land on distinct (line, row, column) entries, so
+            # a gather, a subtraction and a scatter apply them (no sort)
             if e1:
                 Wq = D[lev["o1"]][:, Qp_t]
-                D.index_put_((lev["e1"][:, None, None], P_t[None, :, None], Qn_t[None, None, :]),
-                             -(Lc[lev["e1"]] @ Wq[:, :, N_t] @ Uc[lev["o1"]]), accumulate=True)
+                idx = (lev["e1"][:, None, None], P_t[None, :, None], Qn_t[None, None, :])
+                D[idx] = D[idx] - Lc[lev["e1"]] @ Wq[:, :, N_t] @ Uc[lev["o1"]]
                 newLc = -(Lc[lev["e1"]] @ Wq[:, :, P_t] @ Lc[lev["o1"]])
             if e2:
                 Wq = D[lev["o2"]][:, Qn_t]
-                D.index_put_((lev["e2"][:, None, None], N_t[None, :, None], Qp_t[None, None, :]),
-                             -(Uc[lev["e2"]] @ Wq[:, :, P_t] @ Lc[lev["o2"]]), accumulate=True)
+                idx = (lev["e2"][:, None, None], N_t[None, :, None], Qp_t[None, None, :])
+                D[idx] = D[idx] - Uc[lev["e2"]] @ Wq[:, :, P_t] @ Lc[lev["o2"]]
                 newUc = -(Uc[lev["e2"]] @ Wq[:, :, N_t] @ Uc[lev["o2"]])
             Lc[even[0]] = 0
             if newLc is not None:
