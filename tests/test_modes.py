@@ -225,3 +225,25 @@ def test_krylov_schur_finds_largest_modulus_eigenpairs(k, m):
     for q in range(k):
         x = V[q].numpy()
         assert np.linalg.norm(A @ x - theta[q] * x) < 1e-8 * np.linalg.norm(x) * abs(theta[q])
+
+
+def test_product_component_energy_and_mode_number():
+    """component_energy: the energy fractions eps|E|^2, mu|H|^2 of a mode's
+    raw components (emopt/modes.py:2054-2097); mode numbering is a stub in the
+    reference and raises here."""
+    torch = pytest.importorskip("torch")
+    from emopt_b200.grid import ConstantMaterial3D
+    from emopt_b200.misc import DomainCoordinates
+    from emopt_b200.modes import ModeFullVector
+    dom = DomainCoordinates.from_indices(4, 5, 0, 7, 0, 6, 0.05, 0.05, 0.05)
+    m = ModeFullVector(WL, ConstantMaterial3D(4.0), ConstantMaterial3D(1.0), dom, device=0)
+    rng = np.random.default_rng(9)
+    vec = rng.standard_normal(6 * 6 * 7) + 1j * rng.standard_normal(6 * 6 * 7)
+    m._x = torch.as_tensor(vec.reshape(1, 6, 6, 7))
+    W = m.component_energy(0)
+    raw = [np.sum(np.abs(vec.reshape(6, 42)[q]) ** 2) * (4.0 if q < 3 else 1.0) for q in range(6)]
+    want = [raw[O.COMPONENTS.index(O._PERMUTE["x"][c])] / sum(raw) for c in O.COMPONENTS]
+    np.testing.assert_allclose(W, want, rtol=1e-12)
+    assert sum(W) == pytest.approx(1.0)
+    with pytest.raises(NotImplementedError):
+        m.find_mode_index(0, 0)
