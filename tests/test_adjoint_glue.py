@@ -507,3 +507,25 @@ def test_adjoint_method_mo_combines_objectives():
     assert mo.fom(p) == pytest.approx(np.sum(p ** 2) * 3 * np.sum(p ** 2))
     np.testing.assert_allclose(mo.gradient(p), 2 * 6 * np.sum(p ** 2) * p)
     assert mo.check_gradient(p.copy(), plot=False, verbose=False, fd_step=1e-7) < 1e-5
+
+
+@pytest.mark.parametrize("bc", ["000", "EH0", "HE0"])
+@pytest.mark.parametrize("box", BOXES)
+def test_fdtd_get_field_interp_matches_reference(box, bc):
+    """FDTD.get_field_interp (host numpy, emopt/fdtd.py:1401-1553) on a
+    stand-in holding random fields, against the oracle's restatement."""
+    from types import SimpleNamespace
+
+    from emopt_b200.fdtd import FDTD
+    rng = np.random.default_rng(17)
+    full = dict(zip(A.COMPONENTS, _rand_fields(rng)))
+    Nz, Ny, Nx = SHAPE
+    dx, dy, dz = D
+    sim = SimpleNamespace(_X=(Nx - 1) * dx, _Y=(Ny - 1) * dy, _Z=(Nz - 1) * dz, _dx=dx, _dy=dy, _dz=dz,
+                          _Nx=Nx, _Ny=Ny, _Nz=Nz, _bc=bc)
+    sim.get_field = lambda c, d: np.array(full[c][d.i1:d.i2, d.j1:d.j2, d.k1:d.k2])
+    dom = DomainCoordinates.from_indices(*box, *D)
+    for c in A.COMPONENTS:
+        got = FDTD.get_field_interp(sim, c, dom)
+        want = R.interp(full[c], c, R.Box(*box), bc, D)
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-14)
