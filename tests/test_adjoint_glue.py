@@ -529,3 +529,29 @@ def test_fdtd_get_field_interp_matches_reference(box, bc):
         got = FDTD.get_field_interp(sim, c, dom)
         want = R.interp(full[c], c, R.Box(*box), bc, D)
         np.testing.assert_allclose(got, want, rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("bc", ["000", "0H0", "E0H"])
+def test_fdtd_get_source_power_matches_torch_form(bc):
+    """FDTD.get_source_power (host numpy, emopt/fdtd.py:1555-1667) on a
+    stand-in equals the torch source power of the differentiation form."""
+    import types
+    from types import SimpleNamespace
+
+    from emopt_b200.fdtd import FDTD
+    rng = np.random.default_rng(19)
+    full = dict(zip(A.COMPONENTS, _rand_fields(rng)))
+    Nz, Ny, Nx = SHAPE
+    dx, dy, dz = D
+    w = (2 * dx, 3 * dx, 2 * dy, 0.0, 2 * dz, 2 * dz)
+    sim = SimpleNamespace(_X=(Nx - 1) * dx, _Y=(Ny - 1) * dy, _Z=(Nz - 1) * dz, _dx=dx, _dy=dy, _dz=dz,
+                          _Nx=Nx, _Ny=Ny, _Nz=Nz, _bc=bc, _w_pml=w)
+    sim.get_field = lambda c, d: np.array(full[c][d.i1:d.i2, d.j1:d.j2, d.k1:d.k2])
+    sim.get_field_interp = types.MethodType(FDTD.get_field_interp, sim)
+    P_host = FDTD.get_source_power(sim)
+    fake = SimpleNamespace(dx=dx, dy=dy, dz=dz, _w_pml=w, X=sim._X, Y=sim._Y, Z=sim._Z, bc=bc)
+    planes = A.source_power_planes(fake)
+    grown = [A.grow_domain(dom, SHAPE, D) for dom, _, _ in planes]
+    raws = [torch.as_tensor(np.stack([full[c][g.i1:g.i2, g.j1:g.j2, g.k1:g.k2] for c in A.COMPONENTS]))
+            for g in grown]
+    assert P_host == pytest.approx(float(A.source_power(raws, planes, grown, fake)), rel=1e-12)
