@@ -555,3 +555,31 @@ def test_fdtd_get_source_power_matches_torch_form(bc):
     raws = [torch.as_tensor(np.stack([full[c][g.i1:g.i2, g.j1:g.j2, g.k1:g.k2] for c in A.COMPONENTS]))
             for g in grown]
     assert P_host == pytest.approx(float(A.source_power(raws, planes, grown, fake)), rel=1e-12)
+
+
+def test_source_domain_overlap_is_the_reference_rule():
+    """FDTD._domain_overlap: the reference's local-domain overlap
+    (emopt/fdtd.py:658-708) with the whole grid local, for domains inside,
+    across and outside the grid."""
+    from types import SimpleNamespace
+
+    from emopt_b200.fdtd import FDTD
+    Nz, Ny, Nx = SHAPE
+    sim = SimpleNamespace(_Nz=Nz, _Ny=Ny, _Nx=Nx)
+
+    def reference(d):
+        i0 = j0 = k0 = 0
+        I, J, K = Nz, Ny, Nx
+        if i0 >= d.i2 or i0 + I <= d.i1 or j0 >= d.j2 or j0 + J <= d.j1 or k0 >= d.k2 or k0 + K <= d.k1:
+            return None, None, None, None
+        imax, jmax, kmax = min(i0 + I, d.i2), min(j0 + J, d.j2), min(k0 + K, d.k2)
+        imin, jmin, kmin = max(i0, d.i1), max(j0, d.j1), max(k0, d.k1)
+        return ((imin, jmin, kmin), (imin - i0, jmin - j0, kmin - k0), (imin - d.i1, jmin - d.j1, kmin - d.k1),
+                (imax - imin, jmax - jmin, kmax - kmin))
+
+    rng = np.random.default_rng(23)
+    for _ in range(300):
+        k1, j1, i1 = (int(rng.integers(-4, n + 2)) for n in (Nx, Ny, Nz))
+        k2, j2, i2 = (a + int(rng.integers(1, 8)) for a in (k1, j1, i1))
+        d = DomainCoordinates.from_indices(k1, k2, j1, j2, i1, i2, *D)
+        assert FDTD._domain_overlap(sim, d) == reference(d)
