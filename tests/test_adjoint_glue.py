@@ -583,3 +583,44 @@ def test_source_domain_overlap_is_the_reference_rule():
         k2, j2, i2 = (a + int(rng.integers(1, 8)) for a in (k1, j1, i1))
         d = DomainCoordinates.from_indices(k1, k2, j1, j2, i1, i2, *D)
         assert FDTD._domain_overlap(sim, d) == reference(d)
+
+
+def test_fdtd_build_and_box_update_sample_the_yee_positions():
+    """FDTD.build samples eps at (k+1/2, j, i-1/2), (k, j+1/2, i-1/2), (k, j, i)
+    and mu at (k, j+1/2, i), (k+1/2, j, i), (k+1/2, j+1/2, i-1/2)
+    (emopt/fdtd.py:842-880); update(bbox) re-samples the box's cells only
+    (emopt/fdtd.py:882-992)."""
+    import types
+    from types import SimpleNamespace
+
+    from emopt_b200.fdtd import FDTD
+    from emopt_b200.grid import FunctionMaterial3D
+    Nz, Ny, Nx = SHAPE
+    dx, dy, dz = D
+    state = {"bump": 0.0}
+    fe = lambda x, y, z: (2.0 + np.sin(3 * x) * np.cos(2 * y) + z ** 2 + state["bump"]) + 0.1j * x
+    fm = lambda x, y, z: 1.0 + 0.5 * x * y + 0.25 * z + state["bump"]
+    sim = SimpleNamespace(_Nx=Nx, _Ny=Ny, _Nz=Nz, _dx=dx, _dy=dy, _dz=dz,
+                          _eps=FunctionMaterial3D(fe, dx, dy, dz), _mu=FunctionMaterial3D(fm, dx, dy, dz))
+    for name in ("_eps_x", "_eps_y", "_eps_z", "_mu_x", "_mu_y", "_mu_z"):
+        setattr(sim, name, np.zeros(Nx * Ny * Nz, dtype=np.complex128))
+    sim.build = types.MethodType(FDTD.build, sim)
+    FDTD.build(sim)
+    i, j, k = np.meshgrid(np.arange(Nz), np.arange(Ny), np.arange(Nx), indexing="ij")
+    at = lambda f, sx, sy, sz: f((k + sx) * dx, (j + sy) * dy, (i + sz) * dz)
+    offsets = {"_eps_x": (fe, 0.5, 0.0, -0.5), "_eps_y": (fe, 0.0, 0.5, -0.5), "_eps_z": (fe, 0.0, 0.0, 0.0),
+               "_mu_x": (fm, 0.0, 0.5, 0.0), "_mu_y": (fm, 0.5, 0.0, 0.0), "_mu_z": (fm, 0.5, 0.5, -0.5)}
+    for name, (f, sx, sy, sz) in offsets.items():
+        np.testing.assert_allclose(getattr(sim, name).reshape(SHAPE), at(f, sx, sy, sz), rtol=1e-14)
+    before = {n: getattr(sim, n).reshape(SHAPE).copy() for n in offsets}
+    state["bump"] = 1.0
+    bbox = (3 * dx, 6 * dx, 2 * dy, 4 * dy, 1 * dz, 5 * dz)          # cells k 3-6, j 2-4, i 1-5
+    FDTD.update(sim, bbox)
+    inside = (slice(1, 6), slice(2, 5), slice(3, 7))
+    for name, (f, sx, sy, sz) in offsets.items():
+        now = getattr(sim, name).reshape(SHAPE)
+        np.testing.assert_allclose(now[inside], at(f, sx, sy, sz)[inside], rtol=1e-14)
+        mask = np.ones(SHAPE, bool)
+        mask[inside] = False
+        assert np.array_equal(now[mask], before[name][mask])
+    assert sim._materials_dirty
