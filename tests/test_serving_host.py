@@ -37,3 +37,21 @@ def test_grating_slab_spec():
     assert len(trenches) == 40
     assert all(0.1 - 1e-12 <= x1 - x0 <= 0.4 + 1e-12 for x0, x1, *_ in trenches)
     assert g.src_phase_y > 0
+
+
+def test_request_eps_arrays_voxel_sampling():
+    """eps_arrays: SiO2 background, the boxes in order (later ones win),
+    each Yee component sampled at its own staggered position (the offsets of
+    FDTD.build for eps), on any torch device (here the CPU)."""
+    reqs = S.poisson_stream(3, 20.0, seed=5)
+    for r in reqs:
+        r.shape = (9, 11, 13)                       # small grid, same boxes
+        got = [a.numpy() for a in S.eps_arrays(r, "cpu")]
+        Nz, Ny, Nx = r.shape
+        i, j, k = np.meshgrid(np.arange(Nz), np.arange(Ny), np.arange(Nx), indexing="ij")
+        for c, (sx, sy, sz) in enumerate([(0.5, 0.0, -0.5), (0.0, 0.5, -0.5), (0.0, 0.0, 0.0)]):
+            x, y, z = (k + sx) * r.d, (j + sy) * r.d, (i + sz) * r.d
+            want = np.full(r.shape, S.EPS_SIO2)
+            for x0, x1, y0, y1, z0, z1, v in r.boxes:
+                want = np.where((x >= x0) & (x <= x1) & (y >= y0) & (y <= y1) & (z >= z0) & (z <= z1), v, want)
+            assert np.array_equal(got[c].real, want) and not got[c].imag.any()
