@@ -123,3 +123,16 @@ def test_mode_entry_points_reject_bad_arguments():
                                 1.0) == ct.FDTD_ERR_ARG
     assert lib.FDTD_mode_source(0, None, 0, 3, dummy, 1.0, 0.0, 1.0, 0.0, 1.0, 1.0, 1.0, dummy, dummy,
                                 dummy, b"00", dummy) == ct.FDTD_ERR_ARG
+
+
+def test_integration_snippet_struct_matches_binding():
+    """The ctypes structures shown in INTEGRATION.md declare the fields of the
+    binding, in its order (a shorter struct would be read past its end)."""
+    import re as _re
+    from emopt_b200 import fdtd_ctypes as ct
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    for cls in (ct.SolveOptions, ct.SolveResult):
+        m = _re.search(r"class %s\(Structure\):\s*_fields_ = \[(.*?)\]\n" % cls.__name__, text, _re.S)
+        assert m, cls.__name__
+        names = _re.findall(r'\("(\w+)"', m.group(1))
+        assert names == [f[0] for f in cls._fields_], cls.__name__
