@@ -132,7 +132,8 @@ def test_integration_snippet_struct_matches_binding():
     from emopt_b200 import fdtd_ctypes as ct
     text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     for cls in (ct.SolveOptions, ct.SolveResult):
-        m = _re.search(r"class %s\(Structure\):\s*_fields_ = \[(.*?)\]\n" % cls.__name__, text, _re.S)
+        m = _re.search(r"class %s\(Structure\):\s*_fields_ = \[(.*?)\](?:[ \t]*#[^\n]*)?\n" % cls.__name__,
+                       text, _re.S)
         assert m, cls.__name__
         names = _re.findall(r'\("(\w+)"', m.group(1))
         assert names == [f[0] for f in cls._fields_], cls.__name__
