@@ -137,3 +137,24 @@ def test_integration_snippet_struct_matches_binding():
         assert m, cls.__name__
         names = _re.findall(r'\("(\w+)"', m.group(1))
         assert names == [f[0] for f in cls._fields_], cls.__name__
+
+
+def test_header_compiles_and_struct_sizes_match_binding(tmp_path):
+    """include/emopt_fdtd.h compiles as C and C++, and the structures the
+    ctypes binding mirrors have the same sizes in C."""
+    import shutil
+    import subprocess
+    from emopt_b200 import fdtd_ctypes as ct
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    src = tmp_path / "sizes.c"
+    src.write_text('#include <stdio.h>\n#include "emopt_fdtd.h"\n'
+                   'int main(void) { printf("%zu %zu %zu\\n", sizeof(FDTDSolveOptions), '
+                   'sizeof(FDTDSolveResult), sizeof(FDTDModeLines)); return 0; }\n')
+    exe = tmp_path / "sizes"
+    inc = os.path.join(ROOT, "include")
+    subprocess.run(["gcc", "-Wall", "-Werror", "-I", inc, str(src), "-o", str(exe)], check=True)
+    subprocess.run(["g++", "-fsyntax-only", "-Wall", "-Werror", "-x", "c++", os.path.join(inc, "emopt_fdtd.h")],
+                   check=True)
+    sizes = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert sizes == [ctypes.sizeof(ct.SolveOptions), ctypes.sizeof(ct.SolveResult), ctypes.sizeof(ct.ModeLines)]
