@@ -63,7 +63,7 @@ def test_autograd_transpose_matches_interpolated_dFdx(box):
          for c in A.COMPONENTS}
     F = mm(f)
     F.backward()
-    assert float(F) == pytest.approx(F_ref, rel=1e-13)
+    assert float(F.detach()) == pytest.approx(F_ref, rel=1e-13)
     hol = (torch.conj(raw.grad) / 2).numpy()
     # embed both in full-grid arrays and compare
     for c, comp in enumerate(A.COMPONENTS):
@@ -173,7 +173,7 @@ def test_calc_ydAx_autograd_pseudo_loss(update_mu):
     if update_mu:
         want -= sum(2 * np.sum(np.imag(m.detach().numpy() * take(fwd[c]) * take(adj[c])))
                     for c, m in zip(("Hx", "Hy", "Hz"), mu))
-    assert float(loss) == pytest.approx(want, rel=1e-12)
+    assert float(loss.detach()) == pytest.approx(want, rel=1e-12)
     loss.backward()
     for c, e in zip(("Ex", "Ey", "Ez"), eps):
         np.testing.assert_allclose(e.grad.numpy(), 2 * np.imag(take(fwd[c]) * take(adj[c])), rtol=1e-12)
