@@ -29,8 +29,9 @@ CHECKED = os.path.join(HERE, "FDTD_checked.so")
 # sources whose kernels carry the index checks in the checked library
 CHECKED_SOURCES = ["fdtd_abi.cu", "vec_kernels.cu", "serve_kernels.cu"]
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["fdtd_abi.cu", "step_kernels.cu", "fused_kernels.cu", "tma_kernels.cu",
-           "warp_kernels.cu", "vec_kernels.cu", "vec4_kernels.cu", "stream_kernels.cu", "aux_kernels.cu", "legacy_kernels.cu", "grad_kernels.cu", "serve_kernels.cu", "noalloc.cu", "structured.cu", "modes.cu"]
+SOURCES = ["fdtd_abi.cu", "step_kernels.cu", "vec_kernels.cu", "zmarch_kernels.cu", "aux_kernels.cu",
+           "legacy_kernels.cu", "grad_kernels.cu", "serve_kernels.cu", "noalloc.cu", "structured.cu",
+           "modes.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]

@@ -46,12 +46,6 @@ struct DevBuf {
         owned = true;
         return cudaSuccess;
     }
-    void view(const DevBuf& base, size_t offset, size_t n) {
-        release();
-        p = static_cast<char*>(base.p) + offset;
-        bytes = n;
-        owned = false;
-    }
     void release() {
         if (p && owned) cudaFree(p);
         p = nullptr;
@@ -72,29 +66,25 @@ struct HostSource {
 template <typename T>
 struct Resident {
     int Nx = 0, Ny = 0, Nz = 0, px = 0;
-    DevBuf F[2][6];          // fields; set 1 is the second buffer of the fused kernel
-    DevBuf Hall[2];          // the three H components of a set, contiguous (F[s][3..5] view it)
+    DevBuf F[2][6];          // fields Ex Ey Ez Hx Hy Hz; set 1: the fused step's second set
     DevBuf bE[3], aE[3], bH[3];
     bool mu_uniform[3] = {true, true, true};
     double mu_value[3] = {1, 1, 1};
     bool lossy = false;
     bool coeffs_valid = false;
-    DevBuf psi[2][3][4];
+    DevBuf psi[2][3][4];     // CPML accumulators per set and axis
     DevBuf tab[3][6];
     DevBuf snap[2][6];
     DevBuf stage;            // complex128 staging (one component)
     std::vector<DevBuf> src_ap;    // per source: 6 comps of amp/phase (complex128)
     std::vector<DevBuf> src_coef;  // per source: 6 comps of (a_c, a_s)
     DevBuf steptab, stepbase, flag, err;
-    fdtdb::StepMaps maps[2];
-    bool maps_valid = false;
     DevBuf pwin, pA, pphi, ptimes, pout, pmap;
     int halo = 0;            // planes of halo below and above the fields (z slabs)
     DevBuf psamp;            // z slab: probe samples of all slabs [3][npoints]
 
     void release_all() {
         for (auto& s : F) for (auto& b : s) b.release();
-        for (auto& b : Hall) b.release();
         for (int c = 0; c < 3; c++) { bE[c].release(); aE[c].release(); bH[c].release(); }
         for (auto& s : psi) for (auto& a : s) for (auto& b : a) b.release();
         for (auto& a : tab) for (auto& b : a) b.release();
@@ -104,7 +94,6 @@ struct Resident {
         for (auto& b : src_coef) b.release();
         src_ap.clear(); src_coef.clear();
         steptab.release(); stepbase.release(); flag.release(); err.release();
-        maps_valid = false;
         pwin.release(); pA.release(); pphi.release(); ptimes.release(); pout.release(); pmap.release();
         psamp.release();
         coeffs_valid = false;
@@ -751,7 +740,8 @@ int FDTD_set_precision(FDTDHandle* h, int bits) {
 }
 
 int FDTD_set_kernel(FDTDHandle* h, int which) {
-    if (which < 0 || which > 7) return h->fail(FDTD_ERR_ARG, "kernel must be in 0..7");
+    if (which != 0 && which != 1 && which != 3 && which != 5)
+        return h->fail(FDTD_ERR_ARG, "kernel must be 0 (auto), 1 (scalar), 3 (fused) or 5 (vector)");
     h->kernel = which;
     return FDTD_OK;
 }
@@ -785,59 +775,6 @@ template <typename T> Resident<T>& resident(FDTDHandle* h);
 template <> Resident<float>& resident<float>(FDTDHandle* h) { return h->r32; }
 template <> Resident<double>& resident<double>(FDTDHandle* h) { return h->r64; }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
-// dependency on libcuda).
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess && q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
-    return fn;
-}
-
-// 3D map over one pitched [Nz][Ny][px] component with box (bx, by, 1).
-template <typename T>
-bool encode_plane_map(CUtensorMap* m, void* base, int px, int Ny, int Nz, int bx, int by) {
-    EncodeTiledFn fn = encode_fn();
-    if (!fn) return false;
-    cuuint64_t dims[3] = {(cuuint64_t)px, (cuuint64_t)Ny, (cuuint64_t)Nz};
-    cuuint64_t strides[2] = {(cuuint64_t)px * sizeof(T), (cuuint64_t)px * Ny * sizeof(T)};
-    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
-    cuuint32_t estr[3] = {1, 1, 1};
-    CUtensorMapDataType dt =
-        sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-    return fn(m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
-// Tensor maps for reading set 0 and set 1 (E, H) and the E coefficients.
-template <typename T>
-bool build_maps(FDTDHandle* h, Resident<T>& r) {
-    int TY = fdtdb::tma_tile_rows();
-    for (int s = 0; s < 2; s++)
-        for (int c = 0; c < 3; c++) {
-            if (!encode_plane_map<T>(&r.maps[s].E[c], r.F[s][c].p, r.px, h->Ny, h->Nz, 40, TY + 2))
-                return false;
-            if (!encode_plane_map<T>(&r.maps[s].H[c], r.F[s][3 + c].p, r.px, h->Ny, h->Nz, 36, TY + 1))
-                return false;
-            if (!encode_plane_map<T>(&r.maps[s].B[c], r.bE[c].p, r.px, h->Ny, h->Nz, 32, TY))
-                return false;
-        }
-    return true;
-}
-
 // Allocates the resident arrays for the current grid and PML widths.
 // halo = 1 (z slabs): the six field arrays get one plane below and one above
 // the slab; the interior starts one plane into each array.
@@ -849,22 +786,15 @@ int alloc_resident(FDTDHandle* h, Resident<T>& r, bool two_sets, int halo = 0) {
     r.Nx = h->Nx; r.Ny = h->Ny; r.Nz = h->Nz; r.px = px; r.halo = halo;
     size_t cells = (size_t)h->Nz * h->Ny * px;
     size_t fcells = (size_t)(h->Nz + 2 * halo) * h->Ny * px;
-    for (int s = 0; s < (two_sets ? 2 : 1); s++)
-    {
-        for (int c = 0; c < 3; c++) CK(r.F[s][c].ensure(sizeof(T) * fcells));
-        // H in one block, so that one L2 access-policy window can cover it
-        if (!r.Hall[s].p || r.Hall[s].bytes < 3 * sizeof(T) * fcells) {
-            CK(r.Hall[s].ensure(3 * sizeof(T) * fcells));
-            for (int c = 0; c < 3; c++) r.F[s][3 + c].view(r.Hall[s], c * sizeof(T) * fcells, sizeof(T) * fcells);
-        }
-    }
-    for (int c = 0; c < 3; c++) CK(r.bE[c].ensure(sizeof(T) * cells));
     long long slab[3] = {(long long)h->Nz * h->Ny * (h->w[0] + h->w[1]),
                          (long long)h->Nz * (h->w[2] + h->w[3]) * px,
                          (long long)(h->w[4] + h->w[5]) * h->Ny * px};
-    for (int s = 0; s < (two_sets ? 2 : 1); s++)
+    for (int s = 0; s < (two_sets ? 2 : 1); s++) {
+        for (int c = 0; c < 6; c++) CK(r.F[s][c].ensure(sizeof(T) * fcells));
         for (int a = 0; a < 3; a++)
             for (int q = 0; q < 4; q++) CK(r.psi[s][a][q].ensure(sizeof(T) * (slab[a] ? slab[a] : 1)));
+    }
+    for (int c = 0; c < 3; c++) CK(r.bE[c].ensure(sizeof(T) * cells));
     for (int s = 0; s < 2; s++)
         for (int c = 0; c < 6; c++) CK(r.snap[s][c].ensure(sizeof(T) * cells));
     CK(r.stepbase.ensure(sizeof(long long)));
@@ -1002,7 +932,7 @@ int prepare_sources(FDTDHandle* h, Resident<T>& r, fdtdb::SourceList<T>& list) {
 }
 
 template <typename T>
-fdtdb::GridView<T> make_view(FDTDHandle* h, Resident<T>& r, int set) {
+fdtdb::GridView<T> make_view(FDTDHandle* h, Resident<T>& r, int set = 0) {
     fdtdb::GridView<T> g;
     g.Nx = h->Nx; g.Ny = h->Ny; g.Nz = h->Nz; g.px = r.px;
     g.plane = (long long)h->Ny * r.px;
@@ -1091,28 +1021,15 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
         if (h->bc[a] != '0' && h->bc[a] != 'E' && h->bc[a] != 'H') periodic = true;
     bool small_index = (long long)h->Nz * h->Ny * ((h->Nx + 31) / 32 * 32) < (1LL << 31) &&
                        (long long)h->Nz * h->Ny * (h->w[0] + h->w[1]) < (1LL << 31);
-    // kernel ids: 0 auto, 1 scalar H/E pair, 2 fused CTA tiles (plain loads),
-    // 3 fused CTA tiles (TMA), 4 fused warp tiles, 5 vector H/E pair,
-    // 6 16-byte-vector H/E pair over flattened rows, 7 streaming H/E pair
-    // (row tiles through a bulk-copy ring)
+    // kernel ids: 0 auto (the vector pair), 1 scalar H/E pair, 3 fused
+    // z-marching step, 5 vector H/E pair
     int kid = h->kernel == 0 ? 5 : h->kernel;
     if (periodic || !small_index) kid = 1;
-    if (kid == 3 && encode_fn() == nullptr) kid = 5;
-    if (kid == 6) {
-        int nv;
-        unsigned mg;
-        if (!fdtdb::v16_magic(h->Nx, h->Ny, sizeof(T) == 4 ? 4 : 2, &nv, &mg)) kid = 5;
-    }
-    bool vec = kid == 5;
-    bool v16 = kid == 6;
-    bool strm = kid == 7;
-    bool warp = kid == 4;
-    bool tma = kid == 3;
-    bool fused = kid == 2 || kid == 3 || kid == 4;
+    const bool fused = kid == 3;
+    const bool vec = kid == 5;
     int rc;
     CK(cudaEventRecord(h->ev[2], h->stream));
     if ((rc = alloc_resident<T>(h, r, fused)) != FDTD_OK) return rc;
-    if (tma && !build_maps<T>(h, r)) tma = false;
     CK(cudaMemsetAsync(r.err.p, 0, sizeof(int) * 4, h->stream));
     if (!o->materials_unchanged || !r.coeffs_valid) {
         if ((rc = prepare_materials<T>(h, r)) != FDTD_OK) return rc;
@@ -1166,49 +1083,27 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     pd.nconv = nconv;
 
     long long* sb = dptr<long long>(r.stepbase);
-    int zchunk = h->zchunk > 0 ? h->zchunk : (h->Nz < 32 ? h->Nz : 32);   // TMA kernel
-    int wz = h->zchunk;
-    if (warp && wz <= 0) CK(fdtdb::warp_zchunk<T>(h->Nx, h->Ny, h->Nz, &wz, nullptr));
-    if (tma) wz = zchunk;
     fdtdb::GridView<T> g0 = make_view<T>(h, r, 0);
     fdtdb::GridView<T> g1 = fused ? make_view<T>(h, r, 1) : g0;
-    fdtdb::StreamPlan splan;
-    if (strm && fdtdb::stream_plan<T>(g0, h->zchunk, &splan) != cudaSuccess) {
-        cudaGetLastError();
-        strm = false;
-        vec = true;
-    }
     T* f0[6];
     T* f1[6];
     for (int c = 0; c < 6; c++) {
         f0[c] = dptr<T>(r.F[0][c]);
         f1[c] = fused ? dptr<T>(r.F[1][c]) : f0[c];
     }
-    // Field set that holds the state after `steps` time steps.
+    // field set that holds the state after `steps` time steps
     auto cur_set = [&](long long steps) -> T* const* { return (fused && (steps & 1)) ? f1 : f0; };
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
+    const int zc = h->zchunk > 0 ? h->zchunk : fdtdb::zmarch_chunk(h->Nx, h->Ny, h->Nz, dev_sms);
     auto run = [&](long long n_first, long long count) -> int {
         fdtdb::launch_set_ll(sb, n_first, h->stream);
         launches += 1 + count * (fused ? 1 : 2);
         for (long long q = 0; q < count; q++) {
-            long long n = n_first + q;
-            if (warp) {
-                bool odd = n & 1;
-                CK(fdtdb::launch_step_warp<T>(odd ? g1 : g0, odd ? g0 : g1, odd ? f1 : f0,
-                                              odd ? f0 : f1, src, sb, (int)q, wz, h->stream));
-            } else if (tma) {
-                bool odd = n & 1;
-                CK(fdtdb::launch_step_tma<T>(r.maps[odd ? 1 : 0], odd ? g1 : g0, odd ? g0 : g1,
-                                             odd ? f0 : f1, src, sb, (int)q, zchunk,
-                                             dptr<int>(r.err), h->stream));
-            } else if (fused) {
-                bool odd = n & 1;
-                fdtdb::launch_step_fused<T>(odd ? g1 : g0, odd ? g0 : g1, odd ? f1 : f0,
-                                            odd ? f0 : f1, src, sb, (int)q, h->stream);
-            } else if (strm) {
-                CK(fdtdb::launch_step_stream<T>(g0, f0, src, sb, (int)q, splan, dptr<int>(r.err),
-                                                h->stream));
-            } else if (v16) {
-                CK(fdtdb::launch_step_v16<T>(g0, f0, src, sb, (int)q, h->stream));
+            const bool odd = (n_first + q) & 1;
+            if (fused) {
+                CK(fdtdb::launch_step_zmarch<T>(odd ? g1 : g0, odd ? g0 : g1, odd ? f1 : f0,
+                                                odd ? f0 : f1, src, sb, (int)q, zc, h->stream));
             } else if (vec) {
                 CK(fdtdb::launch_step_vec<T>(g0, f0, src, sb, (int)q, h->stream));
             } else {
@@ -1311,7 +1206,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
     res->device_ms = ms_steps;
     res->total_ms = ms_total;
     res->launches = launches;
-    res->zchunk = (warp || tma) ? wz : (strm ? splan.R : 0);
+    res->zchunk = fused ? zc : 0;
     res->status = FDTD_OK;
     if (!fixed && not_converged()) {
         bool bad = std::isnan(Ach) || std::isinf(Ach) || std::isnan(Pch) || std::isinf(Pch);

@@ -1,7 +1,7 @@
 // kernels.h -- host-side launch wrappers for the CUDA kernels.
 #pragma once
 
-#include <cuda.h>
+#include <cuda_runtime.h>
 
 #include "cell.cuh"
 
@@ -24,71 +24,18 @@ template <typename T>
 cudaError_t launch_half_vec(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
                             const long long* step_base, int off, int half, cudaStream_t st);
 
-// H and E half-steps with one 16-byte vector (4 floats / 2 doubles) of x cells
-// per thread over flattened (row, vector) pairs (vec4_kernels.cu).  Requires
-// non-periodic boundaries; returns cudaErrorInvalidValue when the row split
-// of the flattened index cannot be done exactly for this grid (v16_magic).
+// One fused time step (zmarch_kernels.cu): H and E of every cell, reading the
+// fields and CPML state of (ga, fa) and writing those of (gb, fb); each
+// single-warp CTA marches a 60-cell row segment through zc planes.  Requires
+// non-periodic boundaries and a whole-grid view.
 template <typename T>
-cudaError_t launch_step_v16(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
-                            const long long* step_base, int off, cudaStream_t st);
-bool v16_magic(int Nx, int Ny, int V, int* nvec, unsigned* magic);
+cudaError_t launch_step_zmarch(const GridView<T>& ga, const GridView<T>& gb, T* const* fa,
+                               T* const* fb, const SourceList<T>& src, const long long* step_base,
+                               int off, int zc, cudaStream_t st);
 
-// Streaming H/E pair (stream_kernels.cu): persistent CTAs, row tiles fetched
-// by bulk async copies into a shared-memory ring.  stream_plan fixes the tile
-// rows (rows_hint > 0 caps them), the ring depth and the launch shape for a
-// grid on the current device (once per solve); launch_step_stream runs one
-// time step.  Requires non-periodic boundaries.
-struct StreamPlan {
-    int R, S;              // rows per tile, ring stages
-    int nty, ntiles;       // tiles per plane, tiles in total
-    int nvr;               // 16-byte vectors per row covering Nx
-    unsigned magic;        // q / nvr == umulhi(q, magic) for every q of a tile
-    int stage_bytes, smem, threads, grid;
-    int slot[16];          // byte offset of each array in a stage (this kernel)
-    int hslot[16], eslot[16];
-    int hbox[4], ebox[4];  // planes [0,1) x rows [2,3) reached by M / J sources
-};
-template <typename T>
-cudaError_t stream_plan(const GridView<T>& g, int rows_hint, StreamPlan* plan);
-template <typename T>
-cudaError_t launch_step_stream(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
-                               const long long* step_base, int off, const StreamPlan& plan,
-                               int* err, cudaStream_t st);
-
-// One fused time step reading set A (ga's CPML state, fields fa) and writing
-// set B (gb's CPML state, fields fb).  Requires non-periodic boundaries.
-template <typename T>
-void launch_step_fused(const GridView<T>& ga, const GridView<T>& gb, T* const* fa, T* const* fb,
-                       const SourceList<T>& src, const long long* step_base, int off,
-                       cudaStream_t st);
-
-// TMA descriptors of one read set: E and H components (3D [Nz][Ny][px],
-// boxes 40 x (TY+2) and 36 x (TY+1)) and the E-update coefficients (32 x TY).
-struct StepMaps {
-    CUtensorMap E[3];
-    CUtensorMap H[3];
-    CUtensorMap B[3];
-};
-
-int tma_tile_rows();
-
-// Planes per CTA for the warp-tile kernel: balances the last wave of CTAs
-// (occupancy x SM count slots) against the per-chunk prologue.
-template <typename T>
-cudaError_t warp_zchunk(int Nx, int Ny, int Nz, int* zc, int* slots);
-
-// Fused step on warp-independent register tiles (warp_kernels.cu), zc planes per CTA.
-template <typename T>
-cudaError_t launch_step_warp(const GridView<T>& ga, const GridView<T>& gb, T* const* fa,
-                             T* const* fb, const SourceList<T>& src, const long long* step_base,
-                             int off, int zc, cudaStream_t st);
-
-// Fused step with TMA-staged planes (tma_kernels.cu); *err is set when a
-// bounded wait gives up.
-template <typename T>
-cudaError_t launch_step_tma(const StepMaps& maps, const GridView<T>& ga, const GridView<T>& gb,
-                            T* const* fb, const SourceList<T>& src, const long long* step_base,
-                            int off, int zc, int* err, cudaStream_t st);
+// Planes per z chunk of the fused step: about 32 resident warps per SM on
+// `sms` multiprocessors, at least 4 planes.
+int zmarch_chunk(int Nx, int Ny, int Nz, int sms);
 
 // eps or mu (complex128, dense [Nz][Ny][Nx]) -> pitched update coefficients.
 // b = dt/eps.real, or for lossy media a = (er/dt - ei/2)/(er/dt + ei/2),

@@ -33,7 +33,7 @@ template <> fdtdb::SourceList<double>& slab_src<double>(FDTDHandle* h) { return 
 
 template <typename T>
 fdtdb::GridView<T> slab_view(FDTDHandle* h, Resident<T>& r) {
-    fdtdb::GridView<T> g = make_view<T>(h, r, 0);
+    fdtdb::GridView<T> g = make_view<T>(h, r);
     g.pml[2].off = h->slab_i0;
     g.pml[2].edge_max = h->slab_Nz - h->w[5];
     g.zlo = (char)(h->slab_lo ? 1 : 0);

@@ -63,6 +63,23 @@ __device__ __forceinline__ void vstore(T* p, const T (&d)[V16<T>::N]) {
     *reinterpret_cast<typename V16<T>::type*>(p) = v;
 }
 
+// L2 prefetch distance in planes (0: none).  The warp that updates row j of
+// plane i asks L2 for the same 64-cell segment of plane i + VEC_PREFETCH of
+// the arrays it streams, so that the warp which later updates that plane
+// finds them in L2 (fp32 MMI block: 119.4 instead of 121.0 us per step at
+// distance 2, fp64 199 instead of 205; distance 4 and 8 and one bulk request
+// per array gained less).
+#ifndef VEC_PREFETCH
+#define VEC_PREFETCH 2
+#endif
+
+// p: first cell of the warp's segment; `room` cells of the row's pitch remain
+// from there, so no request leaves the row.
+template <typename T>
+__device__ __forceinline__ void l2_prefetch(const T* p, int lane, int room) {
+    if (2 * lane < room) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p + 2 * lane));
+}
+
 // Does a source box with a non-zero component among comp_base..comp_base+2
 // touch rows [j0, j1), columns [k0, k1) of plane i?
 template <typename T>
@@ -151,6 +168,12 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
     const bool xs = xw && act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
+
+    if (VEC_PREFETCH > 0 && i + VEC_PREFETCH < Nz && j < Ny && xb * 32 * V < g.Nx) {
+        const long long q = (long long)(i + VEC_PREFETCH) * g.plane + (long long)j * px + xb * 32 * V;
+#pragma unroll
+        for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
+    }
 
     // ---- every load of the thread first
     T ex[V], ey[V], ez[V], exj[V], ezj[V], exi[V], eyi[V], hx[V], hy[V], hz[V];
@@ -299,6 +322,14 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
     const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
     const bool xs = xw && act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
     const bool lossy = g.aE[0] != nullptr;
+
+    if (VEC_PREFETCH > 0 && i + VEC_PREFETCH < g.Nz && j < Ny && xb * 32 * V < g.Nx) {
+        const long long q = (long long)(i + VEC_PREFETCH) * g.plane + (long long)j * px + xb * 32 * V;
+#pragma unroll
+        for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
+#pragma unroll
+        for (int c = 0; c < 3; c++) vecb::l2_prefetch<T>(g.bE[c] + q, lane, px - xb * 32 * V);
+    }
 
     // ---- every load of the thread first
     T hx[V], hy[V], hz[V], hxj[V], hzj[V], hxi[V], hyi[V], ex[V], ey[V], ez[V], bx[V], by[V], bz[V];

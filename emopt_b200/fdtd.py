@@ -102,8 +102,7 @@ class FDTD(MaxwellSolver):
     """3D continuous-wave FDTD solver (drop-in for ``emopt.fdtd.FDTD``)."""
 
     # time-stepping kernels of FDTD_solve_cw (include/emopt_fdtd.h, FDTD_set_kernel)
-    KERNELS = {"auto": 0, "scalar": 1, "fused_plain": 2, "fused_tma": 3, "fused_warp": 4,
-               "vector": 5, "vector16": 6, "stream": 7}
+    KERNELS = {"auto": 0, "scalar": 1, "fused": 3, "vector": 5}
 
     def __init__(self, X, Y, Z, dx, dy, dz, wavelength, rtol=1e-6, nconv=None,
                  min_rindex=1.0, complex_eps=False, dist_method="auto",

@@ -19,7 +19,7 @@ from helpers import ROOT
 
 pytestmark = pytest.mark.gpu
 
-SELECT = ("(test_gpu_parity and vector and not vector16) or every_bc or test_fixed_steps "
+SELECT = ("(test_gpu_parity and vector) or every_bc or test_fixed_steps "
           "or test_gpu_serving")
 
 

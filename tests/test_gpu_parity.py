@@ -126,7 +126,7 @@ def test_abi_per_call_field_arrays_match_oracle_each_step():
 
 
 # ------------------------------------------------ device-resident solve
-@pytest.mark.parametrize("kernel", ["stream", "vector16", "vector", "scalar", "fused_plain", "fused_tma", "fused_warp"])
+@pytest.mark.parametrize("kernel", ["fused", "vector", "scalar"])
 @pytest.mark.parametrize("name", list(BOX_KW))
 def test_solve_cw_fp64_matches_golden(name, kernel):
     g = golden(f"box_{name}.npz")
@@ -139,23 +139,24 @@ def test_solve_cw_fp64_matches_golden(name, kernel):
 BC_ALL = [a + b + c for a in "0EH" for b in "0EH" for c in "0EH"]
 
 
+@pytest.mark.parametrize("kernel", ["fused", "vector"])
 @pytest.mark.parametrize("cplx", [False, True])
 @pytest.mark.parametrize("bc", BC_ALL)
-def test_solve_cw_fp64_every_bc_matches_oracle(bc, cplx):
+def test_solve_cw_fp64_every_bc_matches_oracle(bc, cplx, kernel):
     """Every boundary combination {0, E, H}^3, lossless and lossy, through the
-    default stepping kernels: the same tiny blocks on which the oracle equals
+    fused step and the vector pair: the same tiny blocks on which the oracle equals
     the reference core bit for bit (tests/test_oracle.py), solved on the GPU
     in fp64 and compared with the oracle run here."""
     k = BC_ALL.index(bc)
     p = P.random_box(100 + 2 * k + cplx, shape=(5, 6, 7), w_pml=(2, 1, 1, 2, 2, 1), bc=bc,
                      complex_eps=cplx, mu_random=bool(k % 2), edge_source=True, fixed_steps=50)
     ref = oracle_for(p, oracle_lib()).solve(fixed_steps=p.fixed_steps)
-    F, info, _ = solve_gpu(p, "fp64", "auto")
+    F, info, _ = solve_gpu(p, "fp64", kernel)
     assert info["steps"] == ref["steps"]
     assert rel_l2(F, np.stack(ref["fields"])) < 1e-11
 
 
-@pytest.mark.parametrize("kernel", ["vector", "scalar"])
+@pytest.mark.parametrize("kernel", ["fused", "vector", "scalar"])
 @pytest.mark.parametrize("name", list(TAIL_KW))
 def test_row_tail_matches_golden(name, kernel):
     g = golden(f"box_{name}.npz")
@@ -166,12 +167,12 @@ def test_row_tail_matches_golden(name, kernel):
     assert rel_l2(F, g["fields"]) < 1e-11
     # the last x cells, where the tail path and the edge source act
     assert rel_l2(F[..., -4:], g["fields"][..., -4:]) < 1e-11
-    if kernel == "vector":
+    if kernel != "scalar":
         F32, _, _ = solve_gpu(p, "fp32", kernel)
         assert rel_l2(F32, g["fields"]) < 1e-4
 
 
-@pytest.mark.parametrize("kernel", ["stream", "vector16", "vector", "scalar", "fused_plain", "fused_tma", "fused_warp"])
+@pytest.mark.parametrize("kernel", ["fused", "vector", "scalar"])
 def test_solve_cw_fp64_converging_step_count(kernel):
     """Run to rtol = 1e-6: the step count is bit-for-bit the reference's."""
     g = golden("box_converge.npz")
@@ -205,7 +206,7 @@ def test_solve_cw_waveguide_full_field_vs_oracle():
     p = P.waveguide()
     ref = np.stack(oracle_for(p, oracle_lib()).run_fixed_slabs(p.fixed_steps,
                                                                min(32, os.cpu_count() or 1))["fields"])
-    for kern in ("stream", "vector16", "vector", "scalar", "fused_plain", "fused_tma", "fused_warp"):
+    for kern in ("fused", "vector", "scalar"):
         F64, _, _ = solve_gpu(p, "fp64", kern)
         assert rel_l2(F64, ref) < 1e-9, kern
     F32, _, _ = solve_gpu(p, "fp32", "auto")
@@ -214,7 +215,7 @@ def test_solve_cw_waveguide_full_field_vs_oracle():
     assert err32 < 1e-4
 
 
-@pytest.mark.parametrize("kernel", ["stream", "vector16", "vector", "scalar", "fused_tma", "fused_warp"])
+@pytest.mark.parametrize("kernel", ["fused", "vector", "scalar"])
 def test_fp32_box_error(kernel):
     g = golden("box_converge.npz")
     p = P.random_box(seed=11, shape=(10, 12, 15), fixed_steps=None, rtol=1e-6)
