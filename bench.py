@@ -66,6 +66,10 @@ def parse_args():
                          "wavelength 1.55 um, 20-cell CPML)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the fp64 comparison solve")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="default workload: skip the serving-stream sub-object")
+    ap.add_argument("--no-grating", action="store_true",
+                    help="default workload: skip the grating-slab sub-object")
     return ap.parse_args()
 
 
@@ -335,15 +339,37 @@ def run_ours(args):
                               sim64._sources)
         f64 = np.stack([sim64._raw(c, False) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")])
         err = float(np.linalg.norm(fields32 - f64) / np.linalg.norm(f64))
+        # the fp64 solve end to end through the public API (host buffers)
+        sim64._materials_dirty = True
+        t_a = time.perf_counter()
+        sim64.solve_forward()
+        e2e64 = p.ncells * sim64.last_solve["steps"] / (time.perf_counter() - t_a) / 1e9
         alg64 = algorithmic_bytes_per_step(p.shape, p.w_pml, 8)
         step64 = info64["device_ms"] / 1e3 / info64["steps"]
         result["fp64"] = {"value": round(p.ncells * info64["steps"] / (info64["device_ms"] / 1e3) / 1e9, 3),
                           "steps": info64["steps"], "fp32_steps": infos[-1]["steps"],
                           "fp32_rel_l2_vs_fp64": err,
+                          "e2e": {"value": round(e2e64, 3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                                  "d2h_bytes_per_step": d2h},
                           "roofline_frac": round(alg64 / step64 / 1e9 / peak, 4),
                           "speedup_fp32_over_fp64": round(value / (p.ncells * info64["steps"] /
                                                                    (info64["device_ms"] / 1e3) / 1e9), 3)}
         del sim64
+    # ---- the other forms of the path, on the same GPU, after the timed region
+    if rank == 0 and world == 1 and args.workload == "mmi" and args.precision == "fp32":
+        del sim
+        import torch
+        torch.cuda.empty_cache()
+        if not args.no_serving:
+            r = serving_result(local, 512, 20.0, 150.0, 4, first=128)
+            result["serving"] = {"workload": "first 128 requests (by arrival) of the 512-request "
+                                             "Poisson stream at 20/s, seed 3, fp32, rtol 1e-6",
+                                 **{k: v for k, v in r.items() if k != "clocks"},
+                                 "clocks": r["clocks"]}
+            torch.cuda.empty_cache()
+        if not args.no_grating:
+            result["grating"] = {"workload": "grating slab 1201x601x301 (217 M cells), rtol 1e-6",
+                                 **grating_result(local)}
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             result["cpu_baseline"] = cpu_baseline(p)
@@ -357,25 +383,31 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_serving(args):
-    """Serving form: a Poisson stream of CW solves of mixed grids and
-    wavelengths through the continuous-batching engine (FDTD_serve_*)."""
-    world, rank, local = dist_setup(args.gpus)
+def serving_result(local: int, requests: int, rate: float, budget_gb: float, warmup: int,
+                   first: int = 0, request_shape: str = "", fixed_steps: int = 0, world: int = 1,
+                   rank: int = 0):
+    """Serve a Poisson stream of CW solves (config: 512 requests at 20/s,
+    seed 3) through the continuous-batching engine; ``first`` > 0 serves only
+    the first that many requests (by arrival) of the stream.  Returns the
+    result dict (aggregate Gcell-updates/s, latency and service-time
+    percentiles, roofline fraction of the aggregate)."""
     from emopt_b200 import serving as S
     kw = {}
-    if args.request_shape:
-        kw = dict(shape=tuple(int(v) for v in args.request_shape.split(",")), d=0.025,
+    if request_shape:
+        kw = dict(shape=tuple(int(v) for v in request_shape.split(",")), d=0.025,
                   wavelength=1.55, w_pml=20)
-    specs = S.poisson_stream(args.requests, args.rate, seed=3 + rank, **kw)
+    specs = S.poisson_stream(requests, rate, seed=3 + rank, **kw)
+    if first:
+        specs = sorted(specs, key=lambda sp: sp.arrival)[:first]
     for sp in specs:
-        sp.fixed_steps = args.fixed_steps
+        sp.fixed_steps = fixed_steps
     # warm-up: small requests through a throw-away engine (graph, kernels, allocator)
-    if args.warmup > 0:
+    if warmup > 0:
         warm = S.ServeEngine(local, 8e9, 8, 32)
-        S.run_stream(S.poisson_stream(min(args.warmup, 4), 1e9, seed=99, shape=(40, 40, 48), w_pml=8),
+        S.run_stream(S.poisson_stream(min(warmup, 4), 1e9, seed=99, shape=(40, 40, 48), w_pml=8),
                      warm, realtime=False)
         warm.close()
-    eng = S.ServeEngine(local, args.budget_gb * 1e9, 128, 32)
+    eng = S.ServeEngine(local, budget_gb * 1e9, 128, 32)
     barrier(world)
     with ClockSampler(local) as clk:
         out = S.run_stream(specs, eng, realtime=True)
@@ -385,23 +417,45 @@ def run_serving(args):
     (cu,) = barrier_sum([out["cell_updates"]], world)
     value = cu / makespan / 1e9
     steps = [r["steps"] for r in out["results"].values()]
-    result = {
-        "metric": "serving: aggregate Gcell-updates/s with p50/p99 latency (CW-FDTD requests, "
-                  "Poisson arrivals, mixed grids 64^3..384x256x128, fp32, rtol=1e-6)",
-        "value": value, "unit": UNIT, "n_gpus": world, "steps": len(steps), "warmup": min(args.warmup, 4),
-        "ms_per_step": 1e3 * makespan / max(len(steps), 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "serving_stream", "requests": args.requests, "rate_per_s": args.rate,
-                   "budget_gb": args.budget_gb, "steps_per_replay": 32, "seed": 3,
-                   "parallelism": f"replicas{world}"},
+    # algorithmic bytes of every request's time steps (fp32), over the makespan
+    alg = sum(algorithmic_bytes_per_step(sp.shape, [sp.w_pml] * 6, 4) * out["results"][sp.rid]["steps"]
+              for sp in specs)
+    peak, peak_kind = measured_peak()
+    return {
+        "value": value, "unit": UNIT, "requests": len(specs), "makespan_s": makespan,
         "latency_s": {"p50": out["p50"], "p99": out["p99"], "max": float(out["latency"].max()),
                       "mean": float(out["latency"].mean())},
-        "makespan_s": makespan,
+        "service_s": {"p50": out["service_p50"], "p99": out["service_p99"],
+                      "max": float(out["service"].max())},
+        "roofline": {"bound": "hbm", "achieved": alg / makespan / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / makespan / 1e9 / peak, "peak_source": peak_kind,
+                     "note": "aggregate over the makespan (arrival gaps and set-up included)"},
         "time_steps": {"total": int(sum(steps)), "median": float(np.median(steps)),
                        "max": int(max(steps))},
         "nmax_hits": int(sum(1 for r in out["results"].values() if r["status"] != 0)),
         "clocks": clk.summary(),
     }
+
+
+def run_serving(args):
+    """Serving form: a Poisson stream of CW solves of mixed grids and
+    wavelengths through the continuous-batching engine (FDTD_serve_*)."""
+    world, rank, local = dist_setup(args.gpus)
+    r = serving_result(local, args.requests, args.rate, args.budget_gb, args.warmup,
+                       request_shape=args.request_shape, fixed_steps=args.fixed_steps, world=world,
+                       rank=rank)
+    result = {
+        "metric": "serving: aggregate Gcell-updates/s with p50/p99 latency (CW-FDTD requests, "
+                  "Poisson arrivals, mixed grids 64^3..384x256x128, fp32, rtol=1e-6)",
+        "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": r["requests"],
+        "warmup": min(args.warmup, 4), "ms_per_step": 1e3 * r["makespan_s"] / max(r["requests"], 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "serving_stream", "requests": args.requests, "rate_per_s": args.rate,
+                   "budget_gb": args.budget_gb, "steps_per_replay": 32, "seed": 3,
+                   "parallelism": f"replicas{world}"},
+    }
+    result.update({k: v for k, v in r.items() if k not in ("value", "unit")})
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:
@@ -454,12 +508,11 @@ def run_grad(args):
         print(json.dumps(result), flush=True)
 
 
-def run_grating(args):
+def grating_result(local: int, fixed_steps: int = 0):
     """Large single solve: the 1201 x 601 x 301 grating slab (217 M cells),
     float32 and float64 on one GPU, through FDTD_solve_cw with device-built
-    materials and device phasors; reports both rates and the fp32 field
-    error against the fp64 solve."""
-    world, rank, local = dist_setup(args.gpus)
+    materials and device phasors; both rates, their roofline fractions and
+    the fp32 field error against the fp64 solve."""
     import ctypes
     import torch
     from emopt_b200 import fdtd_ctypes as ct
@@ -468,9 +521,10 @@ def run_grating(args):
     dev = torch.device("cuda", local)
     mu_ones = torch.ones(spec0.ncells, dtype=torch.complex128, device=dev)
     out, fields = {}, {}
+    peak, src = measured_peak()
     for prec in (32, 64):
         spec = S.grating_spec(precision=prec)
-        spec.fixed_steps = args.fixed_steps
+        spec.fixed_steps = fixed_steps
         req = S.Request(spec, local, mu_ones)
         req.set_outputs()
         res = ct.SolveResult()
@@ -484,27 +538,33 @@ def run_grating(args):
         out[prec] = {"gcell_updates_per_s": spec.ncells * res.steps / res.device_ms / 1e6,
                      "steps": res.steps, "n_main": res.n_main, "status": st,
                      "device_s": res.device_ms / 1e3, "total_s": res.total_ms / 1e3,
-                     "step_us": step_us,
-                     "roofline_frac": alg / (step_us * 1e-6) / 1e9 / measured_peak()[0]}
+                     "step_us": step_us, "roofline_frac": alg / (step_us * 1e-6) / 1e9 / peak}
         fields[prec] = req.out
         req.out = None
         req.close()
         torch.cuda.empty_cache()
     num = sum(float(torch.sum(torch.abs(a - b) ** 2)) for a, b in zip(fields[32], fields[64]))
     den = sum(float(torch.sum(torch.abs(b) ** 2)) for b in fields[64])
-    peak, src = measured_peak()
+    del fields, mu_ones
+    torch.cuda.empty_cache()
+    return {"value": out[32]["gcell_updates_per_s"], "unit": UNIT, "cells": spec0.ncells,
+            "fp32": out[32], "fp64": out[64], "fp32_rel_l2_vs_fp64": (num / den) ** 0.5,
+            "speedup_fp32_over_fp64": out[32]["gcell_updates_per_s"] / out[64]["gcell_updates_per_s"],
+            "peak_gbs": peak, "peak_source": src}
+
+
+def run_grating(args):
+    world, rank, local = dist_setup(args.gpus)
+    r = grating_result(local, args.fixed_steps)
     result = {
         "metric": "Gcell-updates/s (CW-FDTD, fp32 storage, grating slab 1201x601x301, rtol=1e-6)",
-        "value": out[32]["gcell_updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 0,
-        "ms_per_step": 1e3 * out[32]["device_s"], "higher_is_better": True, "scaling": "weak",
+        "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": 1e3 * r["fp32"]["device_s"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "grating_1201x601x301", "cells": spec0.ncells, "rtol": 1e-6,
+        "config": {"workload": "grating_1201x601x301", "cells": r["cells"], "rtol": 1e-6,
                    "fixed_steps": args.fixed_steps},
-        "fp32": out[32], "fp64": out[64],
-        "fp32_rel_l2_vs_fp64": (num / den) ** 0.5,
-        "speedup_fp32_over_fp64": out[32]["gcell_updates_per_s"] / out[64]["gcell_updates_per_s"],
-        "peak_gbs": peak, "peak_source": src,
     }
+    result.update({k: v for k, v in r.items() if k not in ("value", "unit", "cells")})
     if rank == 0:
         print(json.dumps(result), flush=True)
 

@@ -31,7 +31,7 @@ CHECKED_SOURCES = ["fdtd_abi.cu", "vec_kernels.cu", "serve_kernels.cu"]
 BUILD = os.path.join(HERE, "_build")
 SOURCES = ["fdtd_abi.cu", "step_kernels.cu", "vec_kernels.cu", "zmarch_kernels.cu", "aux_kernels.cu",
            "legacy_kernels.cu", "grad_kernels.cu", "serve_kernels.cu", "noalloc.cu", "structured.cu",
-           "modes.cu"]
+           "modes.cu", "fields_kernels.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]

@@ -13,10 +13,12 @@
 // instead, reserved when the library's device code is loaded on a device and
 // held by every GPU that loads the library until the process exits.
 //
-// Set-up: the first call on a device looks up the array's device address
-// (cudaGetSymbolAddress, with that device current), which also loads the
-// library's device code on that device if nothing else has.  Make that first
-// call before any stream capture.
+// Set-up: every call looks up the array's device address on its device
+// (cudaGetSymbolAddress, with that device current).  The first lookup on a
+// device also loads the library's device code there if nothing else has, so
+// make the first call before any stream capture.  Looking it up each time
+// (cheap once the code is loaded) keeps the address right after a
+// cudaDeviceReset, which reloads the code at another address.
 //
 // Sharing: every call on a device uses the same array, and it keeps the last
 // call's contents.  The conversion reads only the n values that the call
@@ -27,7 +29,6 @@
 
 #include <cstdarg>
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/emopt_fdtd.h"
 #include "kernels.h"
@@ -36,14 +37,10 @@ constexpr long long kScratchBytes = 8ll << 20;  // 8 MiB = FDTD_NOALLOC_MAX_VALU
 static_assert(kScratchBytes == FDTD_NOALLOC_MAX_VALUES * 16ll, "scratch size and header disagree");
 
 // The staging array.  Host code never uses its name as a device address: it
-// asks the runtime for the address on each device (scratch_address below).
+// asks the runtime for the array's address on the current device.
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 namespace {
-
-constexpr int kMaxDevices = 64;
-std::mutex g_lock;
-void* g_addr[kMaxDevices] = {};
 
 int fail(char* msg, int msglen, int status, const char* fmt, ...) __attribute__((format(printf, 4, 5)));
 int fail(char* msg, int msglen, int status, const char* fmt, ...) {
@@ -54,19 +51,6 @@ int fail(char* msg, int msglen, int status, const char* fmt, ...) {
         va_end(ap);
     }
     return status;
-}
-
-// Device address of g_scratch on the current device `dev`, looked up once.
-cudaError_t scratch_address(int dev, void** out) {
-    std::lock_guard<std::mutex> g(g_lock);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e != cudaSuccess) return e;
-        g_addr[dev] = p;
-    }
-    *out = g_addr[dev];
-    return cudaSuccess;
 }
 
 }  // namespace
@@ -86,31 +70,32 @@ extern "C" int FDTD_amp_phase_noalloc(int device, void* stream, fdtd_complex128*
         cudaGetLastError();
         return fail(msg, msglen, FDTD_ERR_NODEVICE, "FDTD_amp_phase_noalloc: no CUDA device");
     }
-    if (device < 0 || device >= ndev || device >= kMaxDevices)
+    if (device < 0 || device >= ndev)
         return fail(msg, msglen, FDTD_ERR_ARG, "FDTD_amp_phase_noalloc: device %d not in [0, %d)",
-                    device, ndev < kMaxDevices ? ndev : kMaxDevices);
+                    device, ndev);
     if (n == 0) return FDTD_OK;
 
     int prev = -1;
     cudaError_t e = cudaGetDevice(&prev);
     if (e == cudaSuccess && prev != device) e = cudaSetDevice(device);
     void* p = nullptr;
-    if (e == cudaSuccess) e = scratch_address(device, &p);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress(&p, g_scratch);
     cudaStream_t st = stream ? (cudaStream_t)stream : cudaStreamPerThread;
     const size_t bytes = sizeof(fdtd_complex128) * (size_t)n;
     const char* where = "set-up";
     if (e == cudaSuccess) {
         where = "copy to device";
-        e = cudaMemcpyAsync(p, a, bytes, cudaMemcpyHostToDevice, st);
+        e = cudaMemcpyAsync(p, a, bytes, cudaMemcpyDefault, st);
     }
     if (e == cudaSuccess) {
         where = "kernel";
+        cudaGetLastError();   // an error left by an earlier call is not this launch's
         fdtdb::launch_amp_phase(reinterpret_cast<fdtdb::c128*>(p), n, st);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
         where = "copy to host";
-        e = cudaMemcpyAsync(a, p, bytes, cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(a, p, bytes, cudaMemcpyDefault, st);
     }
     if (e == cudaSuccess) {
         where = "synchronize";

@@ -225,6 +225,20 @@ libFDTD.FDTD_mode_source.argtypes = [c_int, c_void_p, c_int, c_int, c_void_p, c_
                                      c_void_p, c_void_p, c_char_p, c_void_p]
 libFDTD.FDTD_mode_source.restype = c_int
 
+# field access on the device (fieldops.py)
+libFDTD.FDTD_interp_field.argtypes = [c_int, c_void_p, c_int, c_void_p, POINTER(c_int), c_void_p,
+                                      c_char_p, c_int]
+libFDTD.FDTD_interp_field.restype = c_int
+libFDTD.FDTD_interp_field_T.argtypes = [c_int, c_void_p, c_int, c_void_p, POINTER(c_int), c_void_p,
+                                        c_char_p, c_int]
+libFDTD.FDTD_interp_field_T.restype = c_int
+libFDTD.FDTD_dfdx_interp.argtypes = [c_int, c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_int,
+                                     c_int, c_void_p, c_char_p, c_int]
+libFDTD.FDTD_dfdx_interp.restype = c_int
+libFDTD.FDTD_plane_flux.argtypes = [c_int, c_void_p, c_int, POINTER(c_void_p), POINTER(c_int),
+                                    POINTER(c_int), c_void_p, c_char_p, c_int]
+libFDTD.FDTD_plane_flux.restype = c_int
+
 ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_zchunk",
                  "FDTD_set_precision", "FDTD_set_kernel", "FDTD_solve_cw",
                  "FDTD_amp_phase_noalloc", "FDTD_grad_eps", "FDTD_serve_new",
@@ -235,7 +249,8 @@ ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_
                  "FDTD_slab_capture", "FDTD_slab_finish", "FDTD_structured_values",
                  "FDTD_host_register", "FDTD_host_unregister", "FDTD_mode_last_error",
                  "FDTD_mode_assemble", "FDTD_mode_bmul", "FDTD_mode_lines_gemv", "FDTD_mode_couple",
-                 "FDTD_mode_source")
+                 "FDTD_mode_source", "FDTD_interp_field", "FDTD_interp_field_T", "FDTD_dfdx_interp",
+                 "FDTD_plane_flux")
 
 
 class FDTDError(RuntimeError):

@@ -98,6 +98,14 @@ class ModeMatch:
         return self._k(np.conj(self.Pm)) * (np.conj(self.Eym) * self.x_dot_s - np.conj(self.Exm) * self.y_dot_s)
 
 
+def _on_device(arrays) -> bool:
+    """Are the given derivative arrays CUDA tensors?"""
+    for a in arrays:
+        if a is not None and type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False):
+            return True
+    return False
+
+
 # Where get_field_interp reads each component (offsets (dz, dy, dx) of the
 # samples averaged onto a cell of the Ez grid) and with which weight.
 _TAPS = {
@@ -117,10 +125,17 @@ def interpolated_dFdx_3D(sim, domain, dFdExi, dFdEyi, dFdEzi, dFdHxi, dFdHyi, dF
     shaped like the grown domain.  On a domain touching a symmetric min face
     ('E' or 'H' in ``sim.bc``) the mirrored samples of the interpolation add
     (or, for 'E', subtract) their share to the first plane, as the reference
-    does -- including its use of the y face for Ex under an 'E' letter."""
-    Nz, Ny, Nx = domain.shape
+    does -- including its use of the y face for Ex under an 'E' letter.
+    Given complex CUDA tensors (None for a zero component) it returns CUDA
+    tensors computed on the device."""
     dF = dict(zip(_C, (dFdExi, dFdEyi, dFdEzi, dFdHxi, dFdHyi, dFdHzi)))
     bc = sim.bc
+    if _on_device(dF.values()):
+        # CUDA tensors: the same mapping by the device kernel (FDTD_dfdx_interp)
+        from .fieldops import dfdx_interp
+        grown, out = dfdx_interp(domain, dF, bc)
+        return (grown, *(out[c] for c in _C))
+    Nz, Ny, Nx = domain.shape
     out = []
     for c in _C:
         a = np.zeros((Nz + 2, Ny + 2, Nx + 2), dtype=np.complex128)

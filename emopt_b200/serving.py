@@ -285,16 +285,18 @@ class ServeEngine:
 def run_stream(specs, engine: ServeEngine, realtime: bool = True, keep_fields: bool = False,
                on_done=None):
     """Serve ``specs`` through ``engine`` in arrival order; returns a dict with
-    per-request latency (completion - arrival), the makespan and the aggregate
-    cell updates.  With ``realtime`` the arrivals follow the wall clock;
-    otherwise every request is available at time 0."""
+    per-request latency (completion - arrival) and service time (completion -
+    admission: the time a request spends in the engine, queueing excluded),
+    the makespan and the aggregate cell updates.  With ``realtime`` the
+    arrivals follow the wall clock; otherwise every request is available at
+    time 0."""
     dev = torch.device("cuda", engine.device)
     max_cells = max(s.ncells for s in specs)
     mu_ones = torch.ones(max_cells, dtype=torch.complex128, device=dev)
     pending = list(sorted(specs, key=lambda s: s.arrival))
     waiting = []          # arrived, not yet admitted (FIFO)
     head = None           # the built head of the queue, kept across retries
-    lat, results = {}, {}
+    lat, svc, adm, results = {}, {}, {}, {}
     cell_updates = 0.0
     t0 = time.perf_counter()
     clock = lambda: time.perf_counter() - t0
@@ -307,6 +309,7 @@ def run_stream(specs, engine: ServeEngine, realtime: bool = True, keep_fields: b
                 head = Request(waiting[0], engine.device, mu_ones)
             if not engine.admit(head):
                 break
+            adm[head.spec.rid] = clock()
             waiting.pop(0)
             head = None
         if engine.active:
@@ -315,8 +318,10 @@ def run_stream(specs, engine: ServeEngine, realtime: bool = True, keep_fields: b
                 t = clock()
                 arr = req.spec.arrival if realtime else 0.0
                 lat[req.spec.rid] = t - arr
+                svc[req.spec.rid] = t - adm[req.spec.rid]
                 cell_updates += float(req.spec.ncells) * r["steps"]
                 r["latency"] = t - arr
+                r["service"] = svc[req.spec.rid]
                 if keep_fields:
                     r["fields"] = [a.cpu().numpy() for a in req.out]
                 results[req.spec.rid] = r
@@ -328,6 +333,8 @@ def run_stream(specs, engine: ServeEngine, realtime: bool = True, keep_fields: b
             time.sleep(max(0.0, min(0.005, pending[0].arrival - clock())))
     makespan = clock()
     L = np.array([lat[k] for k in sorted(lat)])
-    return {"latency": L, "results": results, "makespan": makespan, "cell_updates": cell_updates,
-            "p50": float(np.percentile(L, 50)) if len(L) else None,
-            "p99": float(np.percentile(L, 99)) if len(L) else None}
+    S = np.array([svc[k] for k in sorted(svc)])
+    pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None
+    return {"latency": L, "service": S, "results": results, "makespan": makespan,
+            "cell_updates": cell_updates, "p50": pct(L, 50), "p99": pct(L, 99),
+            "service_p50": pct(S, 50), "service_p99": pct(S, 99)}

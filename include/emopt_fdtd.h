@@ -111,10 +111,9 @@ int FDTD_last_error(FDTDHandle *h, char *buf, int buflen);
  * device).  Must precede the first call that touches the device. */
 int FDTD_set_device(FDTDHandle *h, int device);
 
-/* Planes per CTA of the fused time-step kernels, or the largest number of
- * rows per tile of the streaming kernel (0 = chosen from the occupancy or
- * the shared memory, the default).  A tuning knob; results do not depend on
- * it. */
+/* Planes per z chunk of the fused time step (kernel 3; 0 = chosen for about
+ * 32 resident warps per SM, the default).  A tuning knob; results do not
+ * depend on it. */
 int FDTD_set_zchunk(FDTDHandle *h, int planes);
 
 /* Storage/arithmetic precision of FDTD_solve_cw: 64 (default, the reference's
@@ -122,14 +121,12 @@ int FDTD_set_zchunk(FDTDHandle *h, int planes);
  * steady-state fit, probes and outputs stay float64).  Returns a status. */
 int FDTD_set_precision(FDTDHandle *h, int bits);
 
-/* Time-stepping kernel of FDTD_solve_cw: 0 = automatic (default), 1 = H and
- * E kernels with one cell per thread, 2 = fused CTA-tile kernel with plain
- * loads, 3 = fused CTA-tile kernel with TMA-staged planes, 4 = fused kernel on
- * warp-independent register tiles, 5 = H and E kernels with one 2-element
- * vector of x cells per thread, 6 = H and E kernels with one 16-byte vector
- * per thread over flattened rows, 7 = persistent H and E kernels streaming
- * row tiles through a shared-memory ring filled by bulk async copies.
- * Periodic boundaries always use 1. */
+/* Time-stepping kernel of FDTD_solve_cw: 0 = automatic (default: 5), 1 = H
+ * and E kernels with one cell per thread, 3 = one fused H+E kernel per time
+ * step whose warps march up z chunks (reads one field/CPML set, writes the
+ * other), 5 = H and E kernels with one 2-element vector of x cells per
+ * thread.  Other values fail with FDTD_ERR_ARG.  Periodic boundaries always
+ * use 1. */
 int FDTD_set_kernel(FDTDHandle *h, int which);
 
 /* Page-locks (cudaHostRegister, portable) / releases host memory that is
@@ -162,7 +159,7 @@ typedef struct {
     double device_ms;          /* device time of all time steps (CUDA events) */
     double total_ms;           /* device time of the whole call incl. transfers */
     long long launches;        /* kernels this call launched */
-    int zchunk;                /* planes per CTA of a fused kernel, rows per tile of the streaming kernel (else 0) */
+    int zchunk;                /* planes per z chunk of the fused step (kernel 3; else 0) */
     int status;                /* FDTD_OK, FDTD_NMAX or FDTD_NONFINITE */
 } FDTDSolveResult;
 
@@ -298,8 +295,10 @@ int FDTD_slab_finish(FDTDHandle *h, long long n0, long long Tn);
  * 8 MiB device array it stages through. */
 #define FDTD_NOALLOC_MAX_VALUES 524288
 
-/* No counterpart in the reference.  Rewrites the n complex values of the host
- * array a in place as (|a|, -atan2(im, re)) -- the conversion FDTD_add_source
+/* No counterpart in the reference.  Rewrites the n complex values of the
+ * array a (host memory, or memory the device can address: every copy lets the
+ * runtime infer the direction, as FDTD_add_source's do) in place as
+ * (|a|, -atan2(im, re)) -- the conversion FDTD_add_source
  * applies to each source component when calc_phase is true -- on GPU `device`,
  * without allocating any device memory.  It is meant for callers that cannot
  * allocate: a process whose device memory is already committed to a memory
@@ -311,12 +310,54 @@ int FDTD_slab_finish(FDTDHandle *h, long long n0, long long Tn);
  *           default stream; the call returns after that stream has finished.
  *   msg:    optional buffer (msglen bytes) for an error message.
  * n above FDTD_NOALLOC_MAX_VALUES fails with FDTD_ERR_ARG.  Every GPU that
- * loads this library holds the 8 MiB array until the process exits.  The first
- * call on a device looks up the array's address there (set-up); make it before
- * any stream capture.  All calls on a device share the array, so calls that
+ * loads this library holds the 8 MiB array until the process exits.  Each call
+ * looks up the array's address on its device; the first lookup on a device
+ * loads the library's device code there (set-up), so make the first call
+ * before any stream capture.  All calls on a device share the array, so calls that
  * overlap in time (from several host threads) race and must be serialised. */
 int FDTD_amp_phase_noalloc(int device, void *stream, fdtd_complex128 *a, long long n, char *msg,
                            int msglen);
+
+/* ---- field access around a solve, on the device (replaces the numpy forms
+ * of emopt/fdtd.py:1401-1667 and emopt/fomutils.py:1282-1426 when the
+ * phasors live in device memory).  Arrays are complex128 in device memory,
+ * [z][y][x].  geom: 17 ints describing the block an interpolation reads --
+ * origin (i, j, k) in the array, extents (ni, nj, nk), the requested domain's
+ * offset in the block (di, dj, dk) and extents (oi, oj, ok), the array's
+ * dims (NX, NY, NZ), and the sign of the mirrored pad at a symmetric min face
+ * in x and y (-1 'E', +1 'H', 0 none); emopt_b200/fieldops.py derives it the
+ * way the reference slices its arrays.  comp: 0..5 = Ex Ey Ez Hx Hy Hz.
+ * All return a status (message in msg). */
+
+/* The component interpolated onto the Ez grid (get_field_interp,
+ * emopt/fdtd.py:1401-1553): out[oi][oj][ok]. */
+int FDTD_interp_field(int device, void *stream, int comp, const fdtd_complex128 *raw,
+                      const int *geom, fdtd_complex128 *out, char *msg, int msglen);
+
+/* The exact transpose of FDTD_interp_field: the cotangent gout[oi][oj][ok]
+ * mapped onto the block read, graw[ni][nj][nk] (overwritten). */
+int FDTD_interp_field_T(int device, void *stream, int comp, const fdtd_complex128 *gout,
+                        const int *geom, fdtd_complex128 *graw, char *msg, int msglen);
+
+/* interpolated_dFdx_3D of one component (emopt/fomutils.py:1282-1426):
+ * dF[nz][ny][nx] (derivative with respect to the interpolated field on a
+ * domain) -> out[nz+1][ny+1][nx+1] on the domain grown by one cell towards
+ * -x, -y and +z.  qx: the reference's rule for Ex at a symmetric x-min face
+ * (0 none, 1 'H', 2 'E'); qy: sign of its rule for Ey, Hx, Hz at a symmetric
+ * y-min face (0 none). */
+int FDTD_dfdx_interp(int device, void *stream, int comp, const fdtd_complex128 *dF, int nx, int ny,
+                     int nz, int qx, int qy, fdtd_complex128 *out, char *msg, int msglen);
+
+/* Poynting sums of the source power (get_source_power, emopt/fdtd.py:1555-
+ * 1667): for each of nplanes <= 6 planes, sum over its cells of
+ * Re(E1 conj(H2) - E2 conj(H1)) -- (Ey, Hz, Ez, Hy) for axes[p] = 0, (Ex, Hz,
+ * Ez, Hx) for 1, (Ex, Hy, Ey, Hx) for 2 -- every component interpolated as
+ * FDTD_interp_field does.  blocks[6p + c]: component c of plane p's raw
+ * block; geoms: 17 ints per plane.  sums: device memory of at least
+ * 6 + 6 * 148 doubles (partial sums); sums[p] receives plane p's sum, in a
+ * fixed summation order. */
+int FDTD_plane_flux(int device, void *stream, int nplanes, const fdtd_complex128 *const *blocks,
+                    const int *geoms, const int *axes, double *sums, char *msg, int msglen);
 
 /* ---- layered materials on the GPU (replaces the host evaluation of the
  * reference's StructuredMaterial3D with Rectangle and Polygon primitives,

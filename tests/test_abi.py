@@ -20,7 +20,7 @@ def test_library_exports_header_symbols():
     from emopt_b200 import fdtd_ctypes as ct
     lib = ctypes.CDLL(ct.so_path)
     syms = header_symbols()
-    assert len(syms) == 67
+    assert len(syms) == 71
     for s in syms:
         assert hasattr(lib, s), s
     assert set(ct.REFERENCE_SYMBOLS) | set(ct.ADDED_SYMBOLS) == set(syms)
@@ -41,8 +41,9 @@ def test_checked_library_exports_the_same_symbols():
     assert out.returncode == 0 and out.stdout.strip() == "FDTD_checked.so"
 
 
-def test_reference_binding_loads_unchanged():
-    """The reference ctypes argtypes (emopt/fdtd_ctypes.py) bind to this library."""
+def test_binding_declares_reference_symbols():
+    """This package's binding declares the 32 reference symbols (the reference's
+    own binding, unchanged, is driven in tests/test_reference_binding.py)."""
     from emopt_b200 import fdtd_ctypes as ct
     assert len(ct.REFERENCE_SYMBOLS) == 32
     for name in ct.REFERENCE_SYMBOLS:
@@ -125,18 +126,32 @@ def test_mode_entry_points_reject_bad_arguments():
                                 dummy, b"00", dummy) == ct.FDTD_ERR_ARG
 
 
-def test_integration_snippet_struct_matches_binding():
-    """The ctypes structures shown in INTEGRATION.md declare the fields of the
-    binding, in its order (a shorter struct would be read past its end)."""
-    import re as _re
+def test_header_struct_fields_match_binding(tmp_path):
+    """Every field of the ctypes structures exists in the C structures of
+    include/emopt_fdtd.h under the same name and at the same offset (a binding
+    that drifted from the header would read or write the wrong bytes)."""
+    import shutil
+    import subprocess
     from emopt_b200 import fdtd_ctypes as ct
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    for cls in (ct.SolveOptions, ct.SolveResult):
-        m = _re.search(r"class %s\(Structure\):\s*_fields_ = \[(.*?)\](?:[ \t]*#[^\n]*)?\n" % cls.__name__,
-                       text, _re.S)
-        assert m, cls.__name__
-        names = _re.findall(r'\("(\w+)"', m.group(1))
-        assert names == [f[0] for f in cls._fields_], cls.__name__
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    pairs = [("FDTDSolveOptions", ct.SolveOptions), ("FDTDSolveResult", ct.SolveResult),
+             ("FDTDModeLines", ct.ModeLines)]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "emopt_fdtd.h"', 'int main(void) {']
+    for cname, cls in pairs:
+        for f in cls._fields_:
+            lines.append('    printf("%%s %%s %%zu\\n", "%s", "%s", offsetof(%s, %s));' % (cname, f[0], cname, f[0]))
+    lines += ['    return 0;', '}']
+    src = tmp_path / "offsets.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "offsets"
+    subprocess.run(["gcc", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {(a, b): int(c) for a, b, c in (ln.split() for ln in out if ln.strip())}
+    for cname, cls in pairs:
+        for f in cls._fields_:
+            assert got[(cname, f[0])] == getattr(cls, f[0]).offset, (cname, f[0])
 
 
 def test_header_compiles_and_struct_sizes_match_binding(tmp_path):

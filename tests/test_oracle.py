@@ -130,3 +130,20 @@ def test_waveguide_fingerprint_restatement():
     assert np.array_equal(F[idx[:, 0], idx[:, 1], idx[:, 2], idx[:, 3]], g["samples"])
     norms = np.sqrt(np.sum(np.abs(F) ** 2, axis=(1, 2, 3)))
     assert rel_l2(norms, g["norms"]) < 1e-14
+
+
+@pytest.mark.parametrize("seed,shape,nconv,nthreads", [(11, (10, 12, 15), 10, 3), (5, (7, 6, 9), 40, 4)])
+def test_threaded_converging_solve_equals_one_rank(seed, shape, nconv, nthreads):
+    """solve_threads (z slabs on threads, the one-rank probe rule) reproduces
+    the one-rank converging solve bit for bit: step count, probe history,
+    fields.  nconv = 40 on 7 x 6 x 9 cells puts probe points on face ghosts."""
+    p = P.random_box(seed=seed, shape=shape, fixed_steps=None, rtol=1e-6)
+    p.nconv = nconv
+    p.Nmax = 40000
+    o = oracle_for(p, "oracle")
+    ref = o.solve(record=True)
+    thr = oracle_for(p, "oracle").solve_threads(nthreads, record=True)
+    assert thr["n_main"] == ref["n_main"] and thr["steps"] == ref["steps"]
+    assert thr["history"] == ref["history"]
+    for a, b in zip(thr["fields"], ref["fields"]):
+        np.testing.assert_array_equal(a, b)
