@@ -41,16 +41,8 @@ from .misc import DomainCoordinates
 
 COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 
-# Bindings that take raw (device) pointers; the reference-compatible bindings
-# in fdtd_ctypes require numpy arrays for the same symbols.
-_raw = ctypes.CDLL(_ct.so_path)
-_P6 = [ctypes.c_void_p] + [ctypes.c_void_p] * 6
-_raw.FDTD_set_mat_arrays.argtypes = _P6
-_raw.FDTD_set_mat_arrays.restype = None
-_raw.FDTD_set_t0_arrays.argtypes = _P6
-_raw.FDTD_set_t0_arrays.restype = None
-_raw.FDTD_set_t1_arrays.argtypes = _P6
-_raw.FDTD_set_t1_arrays.restype = None
+# array setters that take raw (device) pointers
+_raw = _ct.raw
 
 
 def _ptr(t: torch.Tensor) -> int:

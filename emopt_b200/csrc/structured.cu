@@ -1,8 +1,9 @@
 // structured.cu -- layered materials of rectangles and polygons on the GPU.
 //
 // The material model of the reference's StructuredMaterial3D
-// (src/Grid.cpp:610-874) with Rectangle (src/Grid.cpp:203-300) and Polygon
-// (src/Grid.cpp:300-395) primitives: the z axis is cut into layers at the
+// (src/Grid.cpp:610-874) with Rectangle (src/Grid.cpp:203-300), Polygon
+// (src/Grid.cpp:300-395) and Circle (src/Grid.cpp:141-201) primitives: the z
+// axis is cut into layers at the
 // primitives' z1/z2; inside a layer the value of a Yee cell is the
 // area-weighted average of StructuredMaterial2D (src/Grid.cpp:460-525); along
 // z the value of a cell is the length-weighted average of the layers it spans,
@@ -116,7 +117,22 @@ __device__ bool outline_contains(const Tables& t, int pr, double px, double py) 
     return in;
 }
 
+// A circle (outline count -1): centre and radius in its two outline vertex
+// slots.  Strictly inside when dx^2 + dy^2 < r^2 (src/Grid.cpp:144-149).
+__device__ __forceinline__ bool circle_contains(const Tables& t, int pr, double px, double py) {
+    const int s = t.pinfo[4 * pr];
+    const double dx = px - t.verts[2 * s], dy = py - t.verts[2 * s + 1], r = t.verts[2 * s + 2];
+    return dx * dx + dy * dy < r * r;
+}
+
+__device__ __forceinline__ bool prim_contains(const Tables& t, int pr, double px, double py) {
+    return t.pinfo[4 * pr + 1] < 0 ? circle_contains(t, pr, px, py) : outline_contains(t, pr, px, py);
+}
+
 // Value of layer l at the cell centred on (xd, yd) (src/Grid.cpp:460-525).
+// A circle gives its value to a cell it holds entirely while nothing of the
+// cell is claimed, and otherwise claims nothing: the reference's circle cell
+// overlap is 0 (src/Grid.cpp:167-171).
 __device__ void layer_value(const Tables& t, int l, double xd, double yd, double dx, double dy,
                             double& vr, double& vi, int* err) {
     vr = 0.0;
@@ -140,14 +156,18 @@ __device__ void layer_value(const Tables& t, int l, double xd, double yd, double
     for (int q = t.start[l]; q < t.start[l + 1]; q++) {
         const int pr = t.prims[q];
         const double* v = t.pval + 6 * pr;
-        const bool c1 = outline_contains(t, pr, xmin, ymin), c2 = outline_contains(t, pr, xmax, ymin);
-        const bool c3 = outline_contains(t, pr, xmax, ymax), c4 = outline_contains(t, pr, xmin, ymax);
+        const bool c1 = prim_contains(t, pr, xmin, ymin), c2 = prim_contains(t, pr, xmax, ymin);
+        const bool c3 = prim_contains(t, pr, xmax, ymax), c4 = prim_contains(t, pr, xmin, ymax);
         if (c1 && c2 && c3 && c4 && area / max_area == 1.0) {
             vr = v[0];
             vi = v[1];
             return;
         }
-        if (c1 || c2 || c3 || c4) {
+        if ((c1 || c2 || c3 || c4) && t.pinfo[4 * pr + 1] < 0) {
+            // circle: overlap 0, nothing claimed
+            vr += 0.0 * v[0];
+            vi += 0.0 * v[1];
+        } else if (c1 || c2 || c3 || c4) {
             // the unclaimed pieces minus every convex part of the primitive
             const int p0 = t.pinfo[4 * pr + 2], pn = t.pinfo[4 * pr + 3];
             for (int part = p0; part < p0 + pn; part++) {

@@ -163,6 +163,12 @@ class FDTD(MaxwellSolver):
         self._pin([self._eps_x, self._eps_y, self._eps_z, self._mu_x, self._mu_y, self._mu_z,
                    self._Ex_fwd_t0, self._Ey_fwd_t0, self._Ez_fwd_t0,
                    self._Hx_fwd_t0, self._Hy_fwd_t0, self._Hz_fwd_t0])
+        self._device = None if device is None else int(device)
+        # materials that can be evaluated on the GPU are built there and stay
+        # there (build/update); False keeps the host evaluation
+        self.device_materials = True
+        self._dev_mats = None
+        self._host_mats_stale = False
         if device is not None and libFDTD.FDTD_set_device(h, int(device)) != _ct.FDTD_OK:
             raise _ct.FDTDError(_ct.last_error(h)[1])
         libFDTD.FDTD_set_wavelength(h, wavelength)
@@ -388,13 +394,67 @@ class FDTD(MaxwellSolver):
         Equivalent to what ``build`` samples from material objects
         (``emopt/fdtd.py:842-880``); used when the arrays come from elsewhere.
         """
+        if self._dev_mats is not None:
+            self._register_host_materials()
         targets = (self._eps_x, self._eps_y, self._eps_z, self._mu_x, self._mu_y, self._mu_z)
         for dst, src in zip(targets, list(eps_xyz) + list(mu_xyz)):
             dst[:] = np.asarray(src, dtype=np.complex128).ravel()
         self._materials_dirty = True
 
+    # Yee sampling offsets (sx, sy, sz) of eps_x, eps_y, eps_z, mu_x, mu_y, mu_z
+    # (emopt/fdtd.py:842-880)
+    _YEE = ((0.5, 0.0, -0.5), (0.0, 0.5, -0.5), (0.0, 0.0, 0.0),
+            (0.0, 0.5, 0.0), (0.5, 0.0, 0.0), (0.5, 0.5, -0.5))
+
+    def _device_capable(self):
+        """Can both materials be evaluated on the GPU (layered primitives,
+        constants)?"""
+        from .grid import ConstantMaterial3D, StructuredMaterial3D
+        ok = (StructuredMaterial3D, ConstantMaterial3D)
+        return (getattr(self, "device_materials", False) and isinstance(self._eps, ok)
+                and isinstance(self._mu, ok))
+
+    def _torch_device(self):
+        import torch
+        return torch.device("cuda", self._device if self._device is not None else torch.cuda.current_device())
+
+    def _register_host_materials(self):
+        libFDTD.FDTD_set_mat_arrays(self._libfdtd, self._eps_x, self._eps_y, self._eps_z,
+                                    self._mu_x, self._mu_y, self._mu_z)
+        self._dev_mats = None
+        self._host_mats_stale = False
+
+    def _sync_host_materials(self):
+        """Bring the host material arrays up to date with the device-built ones."""
+        if getattr(self, "_dev_mats", None) is not None and self._host_mats_stale:
+            targets = (self._eps_x, self._eps_y, self._eps_z, self._mu_x, self._mu_y, self._mu_z)
+            for dst, src in zip(targets, self._dev_mats):
+                dst[:] = src.reshape(-1).cpu().numpy()
+            self._host_mats_stale = False
+
+    def _build_device(self):
+        """Evaluate the six Yee-staggered arrays on the GPU, keep them there and
+        hand their device addresses to the library: the solve reads them in
+        place, nothing crosses PCIe (the host arrays follow on demand)."""
+        K, J, I = self._Nx, self._Ny, self._Nz
+        dev = self._torch_device()
+        mats = []
+        for q, (sx, sy, sz) in enumerate(self._YEE):
+            m = self._eps if q < 3 else self._mu
+            mats.append(m.get_values(0, K, 0, J, 0, I, sx=sx, sy=sy, sz=sz, device=dev).contiguous())
+        self._dev_mats = mats
+        _ct.raw.FDTD_set_mat_arrays(self._libfdtd, *[a.data_ptr() for a in mats])
+        self._host_mats_stale = True
+        self._materials_dirty = True
+
     def build(self):
-        """Sample eps/mu at the Yee positions (``emopt/fdtd.py:842-880``)."""
+        """Sample eps/mu at the Yee positions (``emopt/fdtd.py:842-880``); on
+        the GPU, kept there, when both materials can be evaluated there."""
+        if FDTD._device_capable(self):
+            self._build_device()
+            return
+        if getattr(self, "_dev_mats", None) is not None:
+            self._register_host_materials()
         K, J, I = self._Nx, self._Ny, self._Nz
         eps, mu = self._eps, self._mu
         eps.get_values(0, K, 0, J, 0, I, sx=0.5, sy=0.0, sz=-0.5, arr=self._eps_x)
@@ -417,6 +477,17 @@ class FDTD(MaxwellSolver):
         k1, k2 = max(d.k1, 0), min(d.k2, self._Nx)
         if i1 >= i2 or j1 >= j2 or k1 >= k2:
             return
+        if getattr(self, "_dev_mats", None) is not None and FDTD._device_capable(self):
+            # re-sample the box on the GPU into the resident arrays
+            dev = self._torch_device()
+            for q, (sx, sy, sz) in enumerate(self._YEE):
+                m = self._eps if q < 3 else self._mu
+                self._dev_mats[q][i1:i2, j1:j2, k1:k2] = m.get_values(k1, k2, j1, j2, i1, i2, sx=sx, sy=sy,
+                                                                       sz=sz, device=dev)
+            self._host_mats_stale = True
+            self._materials_dirty = True
+            return
+        FDTD._sync_host_materials(self)
         temp = np.zeros((i2 - i1, j2 - j1, k2 - k1), dtype=np.complex128)
         shape = (self._Nz, self._Ny, self._Nx)
         spec = ((self._eps, self._eps_x, (0.5, 0.0, -0.5)), (self._eps, self._eps_y, (0.0, 0.5, -0.5)),
@@ -668,6 +739,7 @@ class FDTD(MaxwellSolver):
 
     def get_A_diag(self):
         """Copies of the six material arrays (``emopt/fdtd.py:1669-1692``)."""
+        FDTD._sync_host_materials(self)
         return tuple(np.copy(a) for a in (self._eps_x, self._eps_y, self._eps_z,
                                           self._mu_x, self._mu_y, self._mu_z))
 
@@ -743,6 +815,7 @@ class FDTD(MaxwellSolver):
     def calc_ydAx(self, Adiag0):
         """y^T dA x with dA = i (eps - eps0) for E and -i (mu - mu0) for H
         (``emopt/fdtd.py:1694-1717``)."""
+        FDTD._sync_host_materials(self)
         eps_x0, eps_y0, eps_z0, mu_x0, mu_y0, mu_z0 = Adiag0
         ydAx = np.zeros(eps_x0.shape, dtype=np.complex128)
         ydAx = ydAx + self._Ex_adj_t0 * 1j * (self._eps_x - eps_x0) * self._Ex_fwd_t0

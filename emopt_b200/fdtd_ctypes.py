@@ -225,6 +225,14 @@ libFDTD.FDTD_mode_source.argtypes = [c_int, c_void_p, c_int, c_int, c_void_p, c_
                                      c_void_p, c_void_p, c_char_p, c_void_p]
 libFDTD.FDTD_mode_source.restype = c_int
 
+# The same library under a second handle whose array setters take raw
+# pointers (device memory included); the reference-compatible bindings above
+# accept numpy arrays only.
+raw = cdll.LoadLibrary(so_path)
+for _name in ("FDTD_set_mat_arrays", "FDTD_set_t0_arrays", "FDTD_set_t1_arrays"):
+    getattr(raw, _name).argtypes = [c_void_p] + [c_void_p] * 6
+    getattr(raw, _name).restype = None
+
 # field access on the device (fieldops.py)
 libFDTD.FDTD_interp_field.argtypes = [c_int, c_void_p, c_int, c_void_p, POINTER(c_int), c_void_p,
                                       c_char_p, c_int]

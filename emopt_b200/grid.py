@@ -3,8 +3,9 @@
 The names and semantics follow ``emopt.grid`` (``emopt/grid.py``, backed by
 the reference's ``Grid.so``, ``src/Grid.cpp``): ``Rectangle`` primitives with a
 material value and a priority ``layer`` (lower wins), and ``Polygon``
-primitives, stacked along z by
-``StructuredMaterial3D.add_primitive(prim, z1, z2)``, and
+primitives, and ``Circle`` primitives with the reference's semantics (a
+cell wholly inside takes the circle's value, a cut cell gets none of it),
+stacked along z by ``StructuredMaterial3D.add_primitive(prim, z1, z2)``, and
 ``ConstantMaterial3D``.  ``get_values`` returns the Yee-cell averages that the
 reference computes -- area-weighted within a z layer, length-weighted across
 layers -- with one CUDA thread per cell (``FDTD_structured_values``), into a
@@ -16,9 +17,8 @@ rectangle after ``add_primitive`` changes the next ``get_values``; the z
 ranges and the priority order are fixed when the primitive is added
 (``src/Grid.cpp:410-433``, ``:627-733``).  ``Polygon`` primitives are simple
 polygons (convex ones evaluated whole, others through a triangulation made
-here); the reference's ``Circle`` (whose overlap is a stub returning 0) is not
-provided; ``FunctionMaterial3D`` samples an analytic ``f(x, y, z)`` at the
-Yee points on the host.
+here); ``FunctionMaterial3D`` samples an analytic ``f(x, y, z)`` at the Yee
+points on the host.
 """
 from __future__ import annotations
 
@@ -87,6 +87,44 @@ class Rectangle(MaterialPrimitive):
         """Strictly inside (``src/Grid.cpp:222-228``)."""
         hw, hh = self._xspan / 2, self._yspan / 2
         return (x > self._x0 - hw) and (x < self._x0 + hw) and (y > self._y0 - hh) and (y < self._y0 + hh)
+
+
+class Circle(MaterialPrimitive):
+    """Circle centred on (x0, y0) with radius r (``emopt/grid.py:330-365``,
+    ``src/Grid.cpp:141-201``).  As in the reference, a circle gives its value
+    only to cells whose four corners lie strictly inside it while no
+    higher-priority primitive has claimed part of the cell; its partial-cell
+    overlap is 0 there (``Circle::get_cell_overlap``), so a cell it only cuts
+    keeps the other primitives' and the background's share."""
+
+    def __init__(self, x0, y0, r):
+        super().__init__()
+        self._x0, self._y0, self._r = float(x0), float(y0), float(r)
+        self._mat = 1.0
+
+    material_value = property(lambda s: s._mat, lambda s, v: setattr(s, "_mat", v))
+
+    def set_material(self, mat):
+        self._mat = mat
+
+    def set_position(self, x0, y0):
+        self._x0, self._y0 = float(x0), float(y0)
+
+    def set_radius(self, r):
+        self._r = float(r)
+
+    def get_x0(self):
+        return self._x0
+
+    def get_y0(self):
+        return self._y0
+
+    def get_r(self):
+        return self._r
+
+    def contains_point(self, x, y):
+        dx, dy = x - self._x0, y - self._y0
+        return dx * dx + dy * dy < self._r * self._r
 
 
 class Polygon(MaterialPrimitive):
@@ -275,8 +313,8 @@ class StructuredMaterial3D(Material3D):
     def add_primitive(self, prim, z1, z2):
         """Add ``prim`` over z1 <= z < z2, splitting layers as needed
         (``src/Grid.cpp:627-733``)."""
-        if not isinstance(prim, (Rectangle, Polygon)):
-            raise TypeError("Rectangle and Polygon primitives are evaluated on the GPU")
+        if not isinstance(prim, (Rectangle, Polygon, Circle)):
+            raise TypeError("Rectangle, Polygon and Circle primitives are evaluated on the GPU")
         self._primitives.append(prim)
         self._zmins.append(z1)
         self._zmaxs.append(z2)
@@ -322,6 +360,15 @@ class StructuredMaterial3D(Material3D):
             start.append(len(flat))
         info, vals, parts, verts = [], [], [], []
         for p in prims:
+            if isinstance(p, Circle):
+                ov = len(verts)
+                verts.extend([[p.get_x0(), p.get_y0()], [p.get_r(), 0.0]])
+                info.append((ov, -1, len(parts), 0))
+                m = complex(p.material_value)
+                r = p.get_r()
+                vals.append((m.real, m.imag, p.get_x0() - r, p.get_x0() + r, p.get_y0() - r,
+                             p.get_y0() + r))
+                continue
             if isinstance(p, Rectangle):
                 x0, x1, y0, y1 = p.bounds()
                 outline = np.array([[x0, y0], [x1, y0], [x1, y1], [x0, y1]])

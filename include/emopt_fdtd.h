@@ -360,12 +360,13 @@ int FDTD_plane_flux(int device, void *stream, int nplanes, const fdtd_complex128
                     const int *geoms, const int *axes, double *sums, char *msg, int msglen);
 
 /* ---- layered materials on the GPU (replaces the host evaluation of the
- * reference's StructuredMaterial3D with Rectangle and Polygon primitives,
- * src/Grid.cpp:203-395 and :460-874, bound by emopt/grid_ctypes.py).
+ * reference's StructuredMaterial3D with Rectangle, Polygon and Circle
+ * primitives, src/Grid.cpp:141-395 and :460-874, bound by emopt/grid_ctypes.py).
  * zs[0..nzs-1]: ascending layer boundaries; layer l (zs[l]..zs[l+1]) holds the
  * primitives layer_prims[layer_start[l] .. layer_start[l+1]) in priority order.
  * Primitive p: prim_info[4p..4p+3] = outline vertex start and count, convex
- * part start and count; prim_vals[6p..6p+5] = Re, Im, xmin, xmax, ymin, ymax
+ * part start and count (a circle: count -1, centre and (radius, 0) in its two
+ * vertex slots, no parts); prim_vals[6p..6p+5] = Re, Im, xmin, xmax, ymin, ymax
  * (outline bounding box).  Part q: parts[2q..2q+1] = vertex start and count
  * (counter-clockwise, convex).  verts: x, y pairs of outlines and parts.
  * Writes the values at fractional indices (k + sx, j + sy, i + sz),

@@ -3,8 +3,8 @@
 Test infrastructure only: the GPU evaluation (emopt_b200/csrc/structured.cu,
 emopt_b200/grid.py) is checked against this.  It restates
 StructuredMaterial3D (src/Grid.cpp:627-826) and StructuredMaterial2D
-(src/Grid.cpp:410-525) for Rectangle and Polygon primitives
-(src/Grid.cpp:203-395) in
+(src/Grid.cpp:410-525) for Rectangle, Polygon and Circle primitives
+(src/Grid.cpp:141-395; a circle is ("circle", x0, y0, r, value)) in
 plain Python, but measures the claimed areas differently from the GPU code
 (which subtracts convex parts piece by piece): each area is integrated
 exactly over vertical slices of the cell, the cross-section at a slice being
@@ -19,6 +19,10 @@ follows the source and is checked on hand-computed cases.
 from __future__ import annotations
 
 
+def _is_circle(prim):
+    return isinstance(prim[0], str) and prim[0] == "circle"
+
+
 def _outline(prim):
     """Counter-clockwise outline of a primitive given as (xmin, xmax, ymin,
     ymax, value) or as (vertices, value)."""
@@ -30,6 +34,13 @@ def _outline(prim):
 
 def _value(prim):
     return prim[4] if len(prim) == 5 else prim[1]
+
+
+def _circle_inside(prim, x, y):
+    """Circle::contains_point (src/Grid.cpp:144-149): strictly inside."""
+    _, x0, y0, r, _ = prim
+    dx, dy = x - x0, y - y0
+    return dx * dx + dy * dy < r * r
 
 
 def _inside(poly, x, y):
@@ -145,6 +156,16 @@ def layer_value(prims, xd, yd, dx, dy):
     val = 0.0
     free = full
     for prim in prims:
+        if _is_circle(prim):
+            # a circle's cell overlap is 0 (src/Grid.cpp:167-171): it gives its
+            # value to a cell it holds entirely while nothing is claimed, and
+            # claims nothing otherwise
+            corners = [_circle_inside(prim, x, y) for x, y in ((x0, y0), (x1, y0), (x1, y1), (x0, y1))]
+            if all(corners) and not taken:
+                return _value(prim)
+            if free == 0:
+                break
+            continue
         poly = _outline(prim)
         corners = [_inside(poly, x0, y0), _inside(poly, x1, y0), _inside(poly, x1, y1),
                    _inside(poly, x0, y1)]

@@ -58,17 +58,21 @@ def _random_polygon(rng):
 
 def _oracle_prim(p):
     m = complex(p.material_value)
+    if isinstance(p, G.Circle):
+        return ("circle", p.get_x0(), p.get_y0(), p.get_r(), m)
     if isinstance(p, G.Rectangle):
         return (*p.bounds(), m)
     return (p.outline().tolist(), m)
 
 
-def _random_layout(seed, n=10, polygons=False):
+def _random_layout(seed, n=10, polygons=False, circles=False):
     rng = np.random.default_rng(seed)
     mat = G.StructuredMaterial3D(4.0, 3.0, 2.0, 0.1, 0.1, 0.1)
     st = LayerStack()
     for q in range(n):
-        if polygons and rng.uniform() < 0.6:
+        if circles and rng.uniform() < 0.4:
+            r = G.Circle(rng.uniform(0, 4), rng.uniform(0, 3), rng.uniform(0.1, 1.5))
+        elif polygons and rng.uniform() < 0.6:
             r = _random_polygon(rng)
         else:
             r = G.Rectangle(rng.uniform(0, 4), rng.uniform(0, 3), rng.uniform(0.05, 2.5), rng.uniform(0.05, 2.0))
@@ -105,7 +109,7 @@ def test_polygon_known_answers():
 
 @pytest.mark.parametrize("seed", range(6))
 def test_layer_tables_match_oracle_stack(seed):
-    mat, st = _random_layout(seed, polygons=True)
+    mat, st = _random_layout(seed, polygons=True, circles=seed % 2 == 1)
     zs, start, flat, info, vals, parts, verts, nprims, nparts, nverts = mat.tables()
     assert list(zs) == st.zs
     assert len(start) == len(st.layers) + 1
@@ -117,9 +121,29 @@ def test_layer_tables_match_oracle_stack(seed):
         for q in range(start[l], start[l + 1]):
             pr = flat[q]
             ov, on = info[pr][0], info[pr][1]
-            got.append((verts[ov:ov + on].tolist(), complex(vals[pr][0], vals[pr][1])))
-        want = [(_outline(p), _value(p)) for p, _ in layer]
+            if on < 0:      # circle: centre and radius
+                got.append(([verts[ov][0], verts[ov][1], verts[ov + 1][0]], complex(vals[pr][0], vals[pr][1])))
+            else:
+                got.append((verts[ov:ov + on].tolist(), complex(vals[pr][0], vals[pr][1])))
+        want = [(([p[1], p[2], p[3]] if isinstance(p[0], str) else _outline(p)), _value(p))
+                for p, _ in layer]
         assert [(np.asarray(a).tolist(), b) for a, b in got] == [(np.asarray(a).tolist(), b) for a, b in want]
+
+
+def test_circle_known_answers():
+    """The reference's circle (src/Grid.cpp:141-201): a cell wholly inside
+    takes its value; a cell it only cuts gets none of it (overlap stub 0) and
+    keeps the background; behind a higher-priority primitive that claimed
+    part of the cell, even a wholly covering circle adds nothing."""
+    m = 6.0 + 0.2j
+    c = ("circle", 0.0, 0.0, 2.0, m)
+    assert layer_value([c], 0.0, 0.0, 1.0, 1.0) == m
+    assert layer_value([c], 2.0, 0.0, 1.0, 1.0) == 1.0           # corners (1.5, +-0.5) inside, cut only
+    rect = (0.0, 5.0, -5.0, 5.0, 3.0)                             # right half of the cell
+    assert layer_value([rect, c], 0.0, 0.0, 1.0, 1.0) == pytest.approx(0.5 * 3 + 0.5)
+    assert layer_value([c, rect], 0.0, 0.0, 1.0, 1.0) == m
+    circ = G.Circle(0.0, 0.0, 2.0)
+    assert circ.contains_point(1.0, 1.0) and not circ.contains_point(2.0, 0.0)
 
 
 def test_self_crossing_polygon_is_rejected():
