@@ -137,324 +137,404 @@ __device__ bool e_fields_ok(const GridView<T>& g, int i, int j, int k0, int lane
 
 }  // namespace vecb
 
-template <typename T>
+// Rows per warp: a warp updates the same 32 vectors of NR consecutive rows
+// j0 .. j0+NR-1 of plane i.  Every load of all rows is issued before any
+// arithmetic, so NR = 2 keeps twice the bytes of one warp in flight; the rows
+// share the loads they have in common (the H update of row j reads E of row
+// j+1, the E update of row j reads H of row j-1).
+template <typename T, int NR = 1>
 __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<T>& f,
                                      const SourceList<T>& src, const long long* step_ctr,
-                                     int off, int i, int j, int xb, int lane) {
+                                     int off, int i, int j0, int xb, int lane) {
     constexpr int V = vecb::V16<T>::N;
     constexpr unsigned FULL = 0xffffffffu;
     const int m = xb * 32 + lane;
     const int k0 = m * V;
-    // Lanes beyond the row still take part in the shuffle below.
-    const bool act0 = j < g.Ny && k0 < g.Nx;
     const int Ny = g.Ny, Nz = g.Nz, px = g.px;
-    const int p = act0 ? (i * Ny + j) * px + k0 : 0;
     const PmlAxis<T>& PX = g.pml[0];
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
-    const int ly0 = slab_local(PY, j, false);   // same for the whole warp
-    const int lz0 = slab_local(PZ, i + PZ.off, true);
+    const int lz0 = slab_local(PZ, i + PZ.off, true);   // same for every row of the warp
+    bool act[NR];
+    int p[NR], ly[NR], lz[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        const int j = j0 + r;
+        // lanes beyond the row still take part in the shuffles below
+        const bool act0 = j < Ny && k0 < g.Nx;
+        p[r] = act0 ? (i * Ny + j) * px + k0 : 0;
+        const int ly0 = slab_local(PY, j, false);
 #ifdef FDTD_BOUNDS_CHECK
-    // a lane whose indices fall outside their arrays records the site and skips
-    const bool act = act0 && vecb::h_fields_ok(g, i, j, k0, lane, p);
-    const int ly = (ly0 >= 0 && act && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
-                                                      (long long)Nz * PY.wsum * px - V + 1, 5)) ? -1 : ly0;
-    const int lz = (lz0 >= 0 && act && !vecb::in_range(g, (long long)(lz0 * Ny + j) * px + k0, 0,
-                                                      (long long)PZ.wsum * Ny * px - V + 1, 6)) ? -1 : lz0;
+        // a lane whose indices fall outside their arrays records the site and skips
+        act[r] = act0 && vecb::h_fields_ok(g, i, j, k0, lane, p[r]);
+        ly[r] = (ly0 >= 0 && act[r] && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
+                                                       (long long)Nz * PY.wsum * px - V + 1, 5)) ? -1 : ly0;
+        lz[r] = (lz0 >= 0 && act[r] && !vecb::in_range(g, (long long)(lz0 * Ny + j) * px + k0, 0,
+                                                       (long long)PZ.wsum * Ny * px - V + 1, 6)) ? -1 : lz0;
 #else
-    const bool act = act0;
-    const int ly = ly0, lz = lz0;
+        act[r] = act0;
+        ly[r] = ly0;
+        lz[r] = lz0;
 #endif
+    }
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
-    const bool xs = xw && act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
 
-    if (VEC_PREFETCH > 0 && i + VEC_PREFETCH < Nz && j < Ny && xb * 32 * V < g.Nx) {
-        const long long q = (long long)(i + VEC_PREFETCH) * g.plane + (long long)j * px + xb * 32 * V;
+    if (VEC_PREFETCH > 0 && i + VEC_PREFETCH < Nz && xb * 32 * V < g.Nx) {
 #pragma unroll
-        for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
+        for (int r = 0; r < NR; r++)
+            if (j0 + r < Ny) {
+                const long long q = (long long)(i + VEC_PREFETCH) * g.plane + (long long)(j0 + r) * px + xb * 32 * V;
+#pragma unroll
+                for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
+            }
     }
 
     // ---- every load of the thread first
-    T ex[V], ey[V], ez[V], exj[V], ezj[V], exi[V], eyi[V], hx[V], hy[V], hz[V];
-    T py0[V], py1[V], pz0[V], pz1[V], px0[V], px1[V];
-    int lxs[V];
-    vecb::vzero<T>(ex); vecb::vzero<T>(ey); vecb::vzero<T>(ez); vecb::vzero<T>(exj); vecb::vzero<T>(ezj);
-    vecb::vzero<T>(exi); vecb::vzero<T>(eyi);
-    T ey_n = T(0), ez_n = T(0);
-    if (act) {
-        vecb::vload<T>(ex, f.c[0] + p); vecb::vload<T>(ey, f.c[1] + p); vecb::vload<T>(ez, f.c[2] + p);
-        if (j + 1 < Ny) { vecb::vload<T>(exj, f.c[0] + p + px); vecb::vload<T>(ezj, f.c[2] + p + px); }
-        if (i + 1 < Nz || g.zhi) { vecb::vload<T>(exi, f.c[0] + p + Ny * px); vecb::vload<T>(eyi, f.c[1] + p + Ny * px); }
-        vecb::vload<T>(hx, f.c[3] + p); vecb::vload<T>(hy, f.c[4] + p); vecb::vload<T>(hz, f.c[5] + p);
-        if (lane == 31 && k0 + V < g.Nx) { ey_n = ld(f.c[1] + p + V); ez_n = ld(f.c[2] + p + V); }
-        if (ly >= 0) {
-            const int s = (i * PY.wsum + ly) * px + k0;
-            vecb::vload<T>(py0, PY.psi[0] + s); vecb::vload<T>(py1, PY.psi[1] + s);
-        }
-        if (lz >= 0) {
-            const int s = (lz * Ny + j) * px + k0;
-            vecb::vload<T>(pz0, PZ.psi[0] + s); vecb::vload<T>(pz1, PZ.psi[1] + s);
-        }
-    }
+    T ex[NR][V], ey[NR][V], ez[NR][V], exj[NR][V], ezj[NR][V], exi[NR][V], eyi[NR][V];
+    T hx[NR][V], hy[NR][V], hz[NR][V];
+    T py0[NR][V], py1[NR][V], pz0[NR][V], pz1[NR][V], px0[NR][V], px1[NR][V];
+    T ey_n[NR], ez_n[NR];
+    int lxs[NR][V];
 #pragma unroll
-    for (int e = 0; e < V; e++) lxs[e] = -1;
-    if (xw) {
+    for (int r = 0; r < NR; r++) {
+        const int j = j0 + r;
+        vecb::vzero<T>(ex[r]); vecb::vzero<T>(ey[r]); vecb::vzero<T>(ez[r]); vecb::vzero<T>(exj[r]);
+        vecb::vzero<T>(ezj[r]); vecb::vzero<T>(exi[r]); vecb::vzero<T>(eyi[r]);
+        ey_n[r] = T(0); ez_n[r] = T(0);
+        if (act[r]) {
+            const int q = p[r];
+            vecb::vload<T>(ex[r], f.c[0] + q); vecb::vload<T>(ey[r], f.c[1] + q); vecb::vload<T>(ez[r], f.c[2] + q);
+            // E of row j+1: the next row's own load, or a load of its own for the last row
+            if (r + 1 == NR && j + 1 < Ny) { vecb::vload<T>(exj[r], f.c[0] + q + px); vecb::vload<T>(ezj[r], f.c[2] + q + px); }
+            if (i + 1 < Nz || g.zhi) { vecb::vload<T>(exi[r], f.c[0] + q + Ny * px); vecb::vload<T>(eyi[r], f.c[1] + q + Ny * px); }
+            vecb::vload<T>(hx[r], f.c[3] + q); vecb::vload<T>(hy[r], f.c[4] + q); vecb::vload<T>(hz[r], f.c[5] + q);
+            if (lane == 31 && k0 + V < g.Nx) { ey_n[r] = ld(f.c[1] + q + V); ez_n[r] = ld(f.c[2] + q + V); }
+            if (ly[r] >= 0) {
+                const int s = (i * PY.wsum + ly[r]) * px + k0;
+                vecb::vload<T>(py0[r], PY.psi[0] + s); vecb::vload<T>(py1[r], PY.psi[1] + s);
+            }
+            if (lz[r] >= 0) {
+                const int s = (lz[r] * Ny + j) * px + k0;
+                vecb::vload<T>(pz0[r], PZ.psi[0] + s); vecb::vload<T>(pz1[r], PZ.psi[1] + s);
+            }
+        }
 #pragma unroll
-    for (int e = 0; e < V; e++) {
-        const int k = k0 + e;
-        lxs[e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
+        for (int e = 0; e < V; e++) lxs[r][e] = -1;
+        if (xw) {
+            const bool xs = act[r] && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
+#pragma unroll
+            for (int e = 0; e < V; e++) {
+                const int k = k0 + e;
+                lxs[r][e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
 #ifdef FDTD_BOUNDS_CHECK
-        if (lxs[e] >= 0 && !vecb::in_range(g, (long long)(i * Ny + j) * PX.wsum + lxs[e], 0,
-                                           (long long)Nz * Ny * PX.wsum, 7))
-            lxs[e] = -1;
+                if (lxs[r][e] >= 0 && !vecb::in_range(g, (long long)(i * Ny + j) * PX.wsum + lxs[r][e], 0,
+                                                      (long long)Nz * Ny * PX.wsum, 7))
+                    lxs[r][e] = -1;
 #endif
-        if (lxs[e] >= 0) {
-            const int s = (i * Ny + j) * PX.wsum + lxs[e];
-            px0[e] = ld(PX.psi[0] + s); px1[e] = ld(PX.psi[1] + s);
+                if (lxs[r][e] >= 0) {
+                    const int s = (i * Ny + j) * PX.wsum + lxs[r][e];
+                    px0[r][e] = ld(PX.psi[0] + s); px1[r][e] = ld(PX.psi[1] + s);
+                }
+            }
         }
     }
-    }
-    T mx[V], my[V], mz[V];
+#pragma unroll
+    for (int r = 0; r + 1 < NR; r++)
+        if (act[r] && j0 + r + 1 < Ny) {
+#pragma unroll
+            for (int e = 0; e < V; e++) { exj[r][e] = ex[r + 1][e]; ezj[r][e] = ez[r + 1][e]; }
+        }
+    T mx[NR][V], my[NR][V], mz[NR][V];
     const bool mu_arr = g.bHarr[0] != nullptr;
-    if (mu_arr && act) { vecb::vload<T>(mx, g.bHarr[0] + p); vecb::vload<T>(my, g.bHarr[1] + p); vecb::vload<T>(mz, g.bHarr[2] + p); }
-    const bool srcb = src.n && vecb::sources_touch<T>(src, 3, i, j, j + 1,
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        if (mu_arr && act[r]) {
+            vecb::vload<T>(mx[r], g.bHarr[0] + p[r]); vecb::vload<T>(my[r], g.bHarr[1] + p[r]);
+            vecb::vload<T>(mz[r], g.bHarr[2] + p[r]);
+        } else {
+#pragma unroll
+            for (int e = 0; e < V; e++) { mx[r][e] = g.bH[0]; my[r][e] = g.bH[1]; mz[r][e] = g.bH[2]; }
+        }
+    }
+    const bool srcb = src.n && vecb::sources_touch<T>(src, 3, i, j0, j0 + NR,
                                                 xb * 32 * V, (xb + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_ctr + off];
 
-    // ---- x neighbour of the last cell: first cell of the next vector
-    {
-        const T a = __shfl_down_sync(FULL, ey[0], 1), b = __shfl_down_sync(FULL, ez[0], 1);
-        if (lane != 31) { ey_n = a; ez_n = b; }
-    }
-    if (!act) return;
-    if (!mu_arr) {
 #pragma unroll
-        for (int e = 0; e < V; e++) { mx[e] = g.bH[0]; my[e] = g.bH[1]; mz[e] = g.bH[2]; }
-    }
-
+    for (int r = 0; r < NR; r++) {
+        const int j = j0 + r;
+        // ---- x neighbour of the last cell: first cell of the next vector
+        {
+            const T a = __shfl_down_sync(FULL, ey[r][0], 1), b = __shfl_down_sync(FULL, ez[r][0], 1);
+            if (lane != 31) { ey_n[r] = a; ez_n[r] = b; }
+        }
+        if (!act[r]) continue;
 #pragma unroll
-    for (int e = 0; e < V; e++) {
-        const T eyx = e + 1 < V ? ey[e + 1] : ey_n;
-        const T ezx = e + 1 < V ? ez[e + 1] : ez_n;
-        const T dEzdy = g.ody * (ezj[e] - ez[e]);
-        const T dEydz = g.odz * (eyi[e] - ey[e]);
-        const T dExdz = g.odz * (exi[e] - ex[e]);
-        const T dEzdx = g.odx * (ezx - ez[e]);
-        const T dEydx = g.odx * (eyx - ey[e]);
-        const T dExdy = g.ody * (exj[e] - ex[e]);
-        T Hx = hx[e] + mx[e] * (dEydz - dEzdy);
-        T Hy = hy[e] + my[e] * (dEzdx - dExdz);
-        T Hz = hz[e] + mz[e] * (dExdy - dEydx);
-        if (xw && lxs[e] >= 0) {
-            const int l = lxs[e];
-            const T kv = ld(PX.kinvH + l), bv = ld(PX.bH + l), cv = ld(PX.cH + l);
-            px0[e] = cv * dEydx + bv * px0[e];
-            px1[e] = cv * dEzdx + bv * px1[e];
-            Hz = Hz - mz[e] * ((px0[e] - dEydx) + dEydx * kv);
-            Hy = Hy + my[e] * ((px1[e] - dEzdx) + dEzdx * kv);
-        }
-        if (ly >= 0) {
-            const T kv = ld(PY.kinvH + ly), bv = ld(PY.bH + ly), cv = ld(PY.cH + ly);
-            py0[e] = cv * dExdy + bv * py0[e];
-            py1[e] = cv * dEzdy + bv * py1[e];
-            Hz = Hz + mz[e] * ((py0[e] - dExdy) + dExdy * kv);
-            Hx = Hx - mx[e] * ((py1[e] - dEzdy) + dEzdy * kv);
-        }
-        if (lz >= 0) {
-            const T kv = ld(PZ.kinvH + lz), bv = ld(PZ.bH + lz), cv = ld(PZ.cH + lz);
-            pz0[e] = cv * dExdz + bv * pz0[e];
-            pz1[e] = cv * dEydz + bv * pz1[e];
-            Hx = Hx + mx[e] * ((pz1[e] - dEydz) + dEydz * kv);
-            Hy = Hy - my[e] * ((pz0[e] - dExdz) + dExdz * kv);
-        }
-        if (srcb && k0 + e < g.Nx)
-            add_sources<T>(src, i, j, k0 + e, 3, T(st.x), T(st.y), Hx, Hy, Hz, false);
-        hx[e] = Hx; hy[e] = Hy; hz[e] = Hz;
-    }
-    vecb::vstore<T>(f.c[3] + p, hx); vecb::vstore<T>(f.c[4] + p, hy); vecb::vstore<T>(f.c[5] + p, hz);
-    if (ly >= 0) {
-        const int s = (i * PY.wsum + ly) * px + k0;
-        vecb::vstore<T>(PY.psi[0] + s, py0); vecb::vstore<T>(PY.psi[1] + s, py1);
-    }
-    if (lz >= 0) {
-        const int s = (lz * Ny + j) * px + k0;
-        vecb::vstore<T>(PZ.psi[0] + s, pz0); vecb::vstore<T>(PZ.psi[1] + s, pz1);
-    }
-    if (xw) {
-#pragma unroll
-        for (int e = 0; e < V; e++)
-            if (lxs[e] >= 0) {
-                const int s = (i * Ny + j) * PX.wsum + lxs[e];
-                PX.psi[0][s] = px0[e]; PX.psi[1][s] = px1[e];
+        for (int e = 0; e < V; e++) {
+            const T eyx = e + 1 < V ? ey[r][e + 1] : ey_n[r];
+            const T ezx = e + 1 < V ? ez[r][e + 1] : ez_n[r];
+            const T dEzdy = g.ody * (ezj[r][e] - ez[r][e]);
+            const T dEydz = g.odz * (eyi[r][e] - ey[r][e]);
+            const T dExdz = g.odz * (exi[r][e] - ex[r][e]);
+            const T dEzdx = g.odx * (ezx - ez[r][e]);
+            const T dEydx = g.odx * (eyx - ey[r][e]);
+            const T dExdy = g.ody * (exj[r][e] - ex[r][e]);
+            T Hx = hx[r][e] + mx[r][e] * (dEydz - dEzdy);
+            T Hy = hy[r][e] + my[r][e] * (dEzdx - dExdz);
+            T Hz = hz[r][e] + mz[r][e] * (dExdy - dEydx);
+            if (xw && lxs[r][e] >= 0) {
+                const int l = lxs[r][e];
+                const T kv = ld(PX.kinvH + l), bv = ld(PX.bH + l), cv = ld(PX.cH + l);
+                px0[r][e] = cv * dEydx + bv * px0[r][e];
+                px1[r][e] = cv * dEzdx + bv * px1[r][e];
+                Hz = Hz - mz[r][e] * ((px0[r][e] - dEydx) + dEydx * kv);
+                Hy = Hy + my[r][e] * ((px1[r][e] - dEzdx) + dEzdx * kv);
             }
+            if (ly[r] >= 0) {
+                const int l = ly[r];
+                const T kv = ld(PY.kinvH + l), bv = ld(PY.bH + l), cv = ld(PY.cH + l);
+                py0[r][e] = cv * dExdy + bv * py0[r][e];
+                py1[r][e] = cv * dEzdy + bv * py1[r][e];
+                Hz = Hz + mz[r][e] * ((py0[r][e] - dExdy) + dExdy * kv);
+                Hx = Hx - mx[r][e] * ((py1[r][e] - dEzdy) + dEzdy * kv);
+            }
+            if (lz[r] >= 0) {
+                const int l = lz[r];
+                const T kv = ld(PZ.kinvH + l), bv = ld(PZ.bH + l), cv = ld(PZ.cH + l);
+                pz0[r][e] = cv * dExdz + bv * pz0[r][e];
+                pz1[r][e] = cv * dEydz + bv * pz1[r][e];
+                Hx = Hx + mx[r][e] * ((pz1[r][e] - dEydz) + dEydz * kv);
+                Hy = Hy - my[r][e] * ((pz0[r][e] - dExdz) + dExdz * kv);
+            }
+            if (srcb && k0 + e < g.Nx)
+                add_sources<T>(src, i, j, k0 + e, 3, T(st.x), T(st.y), Hx, Hy, Hz, false);
+            hx[r][e] = Hx; hy[r][e] = Hy; hz[r][e] = Hz;
+        }
+        const int q = p[r];
+        vecb::vstore<T>(f.c[3] + q, hx[r]); vecb::vstore<T>(f.c[4] + q, hy[r]); vecb::vstore<T>(f.c[5] + q, hz[r]);
+        if (ly[r] >= 0) {
+            const int s = (i * PY.wsum + ly[r]) * px + k0;
+            vecb::vstore<T>(PY.psi[0] + s, py0[r]); vecb::vstore<T>(PY.psi[1] + s, py1[r]);
+        }
+        if (lz[r] >= 0) {
+            const int s = (lz[r] * Ny + j) * px + k0;
+            vecb::vstore<T>(PZ.psi[0] + s, pz0[r]); vecb::vstore<T>(PZ.psi[1] + s, pz1[r]);
+        }
+        if (xw) {
+#pragma unroll
+            for (int e = 0; e < V; e++)
+                if (lxs[r][e] >= 0) {
+                    const int s = (i * Ny + j) * PX.wsum + lxs[r][e];
+                    PX.psi[0][s] = px0[r][e]; PX.psi[1][s] = px1[r][e];
+                }
+        }
     }
 }
 
-template <typename T>
+template <typename T, int NR = 1>
 __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<T>& f,
                                      const SourceList<T>& src, const long long* step_ctr,
-                                     int off, int i, int j, int xb, int lane) {
+                                     int off, int i, int j0, int xb, int lane) {
     constexpr int V = vecb::V16<T>::N;
     constexpr unsigned FULL = 0xffffffffu;
     const int m = xb * 32 + lane;
     const int k0 = m * V;
-    const bool act0 = j < g.Ny && k0 < g.Nx;
     const int Ny = g.Ny, px = g.px;
-    const int p = act0 ? (i * Ny + j) * px + k0 : 0;
     const PmlAxis<T>& PX = g.pml[0];
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
-    const int ly0 = slab_local(PY, j, false);   // same for the whole warp
-    const int lz0 = slab_local(PZ, i + PZ.off, true);
+    const int lz0 = slab_local(PZ, i + PZ.off, true);   // same for every row of the warp
+    bool act[NR];
+    int p[NR], ly[NR], lz[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        const int j = j0 + r;
+        const bool act0 = j < Ny && k0 < g.Nx;
+        p[r] = act0 ? (i * Ny + j) * px + k0 : 0;
+        const int ly0 = slab_local(PY, j, false);
 #ifdef FDTD_BOUNDS_CHECK
-    const bool act = act0 && vecb::e_fields_ok(g, i, j, k0, lane, p);
-    const int ly = (ly0 >= 0 && act && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
-                                                      (long long)g.Nz * PY.wsum * px - V + 1, 15)) ? -1 : ly0;
-    const int lz = (lz0 >= 0 && act && !vecb::in_range(g, (long long)(lz0 * Ny + j) * px + k0, 0,
-                                                      (long long)PZ.wsum * Ny * px - V + 1, 16)) ? -1 : lz0;
+        act[r] = act0 && vecb::e_fields_ok(g, i, j, k0, lane, p[r]);
+        ly[r] = (ly0 >= 0 && act[r] && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
+                                                       (long long)g.Nz * PY.wsum * px - V + 1, 15)) ? -1 : ly0;
+        lz[r] = (lz0 >= 0 && act[r] && !vecb::in_range(g, (long long)(lz0 * Ny + j) * px + k0, 0,
+                                                       (long long)PZ.wsum * Ny * px - V + 1, 16)) ? -1 : lz0;
 #else
-    const bool act = act0;
-    const int ly = ly0, lz = lz0;
+        act[r] = act0;
+        ly[r] = ly0;
+        lz[r] = lz0;
 #endif
+    }
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
-    const bool xs = xw && act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
     const bool lossy = g.aE[0] != nullptr;
 
-    if (VEC_PREFETCH > 0 && i + VEC_PREFETCH < g.Nz && j < Ny && xb * 32 * V < g.Nx) {
-        const long long q = (long long)(i + VEC_PREFETCH) * g.plane + (long long)j * px + xb * 32 * V;
+    if (VEC_PREFETCH > 0 && i + VEC_PREFETCH < g.Nz && xb * 32 * V < g.Nx) {
 #pragma unroll
-        for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
+        for (int r = 0; r < NR; r++)
+            if (j0 + r < Ny) {
+                const long long q = (long long)(i + VEC_PREFETCH) * g.plane + (long long)(j0 + r) * px + xb * 32 * V;
 #pragma unroll
-        for (int c = 0; c < 3; c++) vecb::l2_prefetch<T>(g.bE[c] + q, lane, px - xb * 32 * V);
+                for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
+#pragma unroll
+                for (int c = 0; c < 3; c++) vecb::l2_prefetch<T>(g.bE[c] + q, lane, px - xb * 32 * V);
+            }
     }
 
     // ---- every load of the thread first
-    T hx[V], hy[V], hz[V], hxj[V], hzj[V], hxi[V], hyi[V], ex[V], ey[V], ez[V], bx[V], by[V], bz[V];
-    T py2[V], py3[V], pz2[V], pz3[V], px2[V], px3[V], ax[V], ay[V], az[V];
-    int lxs[V];
-    vecb::vzero<T>(hy); vecb::vzero<T>(hz);
-    T hy_p = T(0), hz_p = T(0);
-    if (act) {
-        vecb::vload<T>(hx, f.c[3] + p); vecb::vload<T>(hy, f.c[4] + p); vecb::vload<T>(hz, f.c[5] + p);
-        vecb::vload<T>(ex, f.c[0] + p); vecb::vload<T>(ey, f.c[1] + p); vecb::vload<T>(ez, f.c[2] + p);
-        vecb::vload<T>(bx, g.bE[0] + p); vecb::vload<T>(by, g.bE[1] + p); vecb::vload<T>(bz, g.bE[2] + p);
-        if (j > 0) { vecb::vload<T>(hxj, f.c[3] + p - px); vecb::vload<T>(hzj, f.c[5] + p - px); }
-        if (i > 0 || g.zlo) { vecb::vload<T>(hxi, f.c[3] + p - Ny * px); vecb::vload<T>(hyi, f.c[4] + p - Ny * px); }
-        if (lane == 0 && k0 > 0) { hy_p = ld(f.c[4] + p - 1); hz_p = ld(f.c[5] + p - 1); }
-        if (ly >= 0) {
-            const int s = (i * PY.wsum + ly) * px + k0;
-            vecb::vload<T>(py2, PY.psi[2] + s); vecb::vload<T>(py3, PY.psi[3] + s);
-        }
-        if (lz >= 0) {
-            const int s = (lz * Ny + j) * px + k0;
-            vecb::vload<T>(pz2, PZ.psi[2] + s); vecb::vload<T>(pz3, PZ.psi[3] + s);
-        }
-        if (lossy) { vecb::vload<T>(ax, g.aE[0] + p); vecb::vload<T>(ay, g.aE[1] + p); vecb::vload<T>(az, g.aE[2] + p); }
-    }
+    T hx[NR][V], hy[NR][V], hz[NR][V], hxj[NR][V], hzj[NR][V], hxi[NR][V], hyi[NR][V];
+    T ex[NR][V], ey[NR][V], ez[NR][V], bx[NR][V], by[NR][V], bz[NR][V];
+    T py2[NR][V], py3[NR][V], pz2[NR][V], pz3[NR][V], px2[NR][V], px3[NR][V], ax[NR][V], ay[NR][V], az[NR][V];
+    T hy_p[NR], hz_p[NR];
+    int lxs[NR][V];
 #pragma unroll
-    for (int e = 0; e < V; e++) lxs[e] = -1;
-    if (xw) {
+    for (int r = 0; r < NR; r++) {
+        const int j = j0 + r;
+        vecb::vzero<T>(hy[r]); vecb::vzero<T>(hz[r]);
+        hy_p[r] = T(0); hz_p[r] = T(0);
+        if (act[r]) {
+            const int q = p[r];
+            vecb::vload<T>(hx[r], f.c[3] + q); vecb::vload<T>(hy[r], f.c[4] + q); vecb::vload<T>(hz[r], f.c[5] + q);
+            vecb::vload<T>(ex[r], f.c[0] + q); vecb::vload<T>(ey[r], f.c[1] + q); vecb::vload<T>(ez[r], f.c[2] + q);
+            vecb::vload<T>(bx[r], g.bE[0] + q); vecb::vload<T>(by[r], g.bE[1] + q); vecb::vload<T>(bz[r], g.bE[2] + q);
+            // H of row j-1: the previous row's own load, or a load of its own for the first row
+            if (r == 0 && j > 0) { vecb::vload<T>(hxj[r], f.c[3] + q - px); vecb::vload<T>(hzj[r], f.c[5] + q - px); }
+            if (i > 0 || g.zlo) { vecb::vload<T>(hxi[r], f.c[3] + q - Ny * px); vecb::vload<T>(hyi[r], f.c[4] + q - Ny * px); }
+            if (lane == 0 && k0 > 0) { hy_p[r] = ld(f.c[4] + q - 1); hz_p[r] = ld(f.c[5] + q - 1); }
+            if (ly[r] >= 0) {
+                const int s = (i * PY.wsum + ly[r]) * px + k0;
+                vecb::vload<T>(py2[r], PY.psi[2] + s); vecb::vload<T>(py3[r], PY.psi[3] + s);
+            }
+            if (lz[r] >= 0) {
+                const int s = (lz[r] * Ny + j) * px + k0;
+                vecb::vload<T>(pz2[r], PZ.psi[2] + s); vecb::vload<T>(pz3[r], PZ.psi[3] + s);
+            }
+            if (lossy) {
+                vecb::vload<T>(ax[r], g.aE[0] + q); vecb::vload<T>(ay[r], g.aE[1] + q); vecb::vload<T>(az[r], g.aE[2] + q);
+            }
+        }
 #pragma unroll
-    for (int e = 0; e < V; e++) {
-        const int k = k0 + e;
-        lxs[e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
+        for (int e = 0; e < V; e++) lxs[r][e] = -1;
+        if (xw) {
+            const bool xs = act[r] && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
+#pragma unroll
+            for (int e = 0; e < V; e++) {
+                const int k = k0 + e;
+                lxs[r][e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
 #ifdef FDTD_BOUNDS_CHECK
-        if (lxs[e] >= 0 && !vecb::in_range(g, (long long)(i * Ny + j) * PX.wsum + lxs[e], 0,
-                                           (long long)g.Nz * Ny * PX.wsum, 17))
-            lxs[e] = -1;
+                if (lxs[r][e] >= 0 && !vecb::in_range(g, (long long)(i * Ny + j) * PX.wsum + lxs[r][e], 0,
+                                                      (long long)g.Nz * Ny * PX.wsum, 17))
+                    lxs[r][e] = -1;
 #endif
-        if (lxs[e] >= 0) {
-            const int s = (i * Ny + j) * PX.wsum + lxs[e];
-            px2[e] = ld(PX.psi[2] + s); px3[e] = ld(PX.psi[3] + s);
+                if (lxs[r][e] >= 0) {
+                    const int s = (i * Ny + j) * PX.wsum + lxs[r][e];
+                    px2[r][e] = ld(PX.psi[2] + s); px3[r][e] = ld(PX.psi[3] + s);
+                }
+            }
         }
     }
-    }
-    const bool srcb = src.n && vecb::sources_touch<T>(src, 0, i, j, j + 1,
+#pragma unroll
+    for (int r = 1; r < NR; r++)
+        if (act[r]) {
+#pragma unroll
+            for (int e = 0; e < V; e++) { hxj[r][e] = hx[r - 1][e]; hzj[r][e] = hz[r - 1][e]; }
+        }
+    const bool srcb = src.n && vecb::sources_touch<T>(src, 0, i, j0, j0 + NR,
                                                 xb * 32 * V, (xb + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_ctr + off];
 
-    // ---- x neighbour of the first cell: last cell of the previous vector
-    {
-        const T a = __shfl_up_sync(FULL, hy[V - 1], 1), b = __shfl_up_sync(FULL, hz[V - 1], 1);
-        if (lane != 0) { hy_p = a; hz_p = b; }
-    }
-    if (!act) return;
-    if (k0 == 0) { hy_p = h_min_ghost<T>(g.bc[0], hy[0], T(0)); hz_p = h_min_ghost<T>(g.bc[0], hz[0], T(0)); }
-    if (j == 0) {
 #pragma unroll
-        for (int e = 0; e < V; e++) { hxj[e] = h_min_ghost<T>(g.bc[1], hx[e], T(0)); hzj[e] = h_min_ghost<T>(g.bc[1], hz[e], T(0)); }
-    }
-    if (i == 0 && !g.zlo) {
+    for (int r = 0; r < NR; r++) {
+        const int j = j0 + r;
+        // ---- x neighbour of the first cell: last cell of the previous vector
+        {
+            const T a = __shfl_up_sync(FULL, hy[r][V - 1], 1), b = __shfl_up_sync(FULL, hz[r][V - 1], 1);
+            if (lane != 0) { hy_p[r] = a; hz_p[r] = b; }
+        }
+        if (!act[r]) continue;
+        if (k0 == 0) { hy_p[r] = h_min_ghost<T>(g.bc[0], hy[r][0], T(0)); hz_p[r] = h_min_ghost<T>(g.bc[0], hz[r][0], T(0)); }
+        if (j == 0) {
 #pragma unroll
-        for (int e = 0; e < V; e++) { hxi[e] = h_min_ghost<T>(g.bc[2], hx[e], T(0)); hyi[e] = h_min_ghost<T>(g.bc[2], hy[e], T(0)); }
-    }
-
-#pragma unroll
-    for (int e = 0; e < V; e++) {
-        const T hyx = e > 0 ? hy[e - 1] : hy_p;
-        const T hzx = e > 0 ? hz[e - 1] : hz_p;
-        const T dHzdy = g.ody * (hz[e] - hzj[e]);
-        const T dHydz = g.odz * (hy[e] - hyi[e]);
-        const T dHxdz = g.odz * (hx[e] - hxi[e]);
-        const T dHzdx = g.odx * (hz[e] - hzx);
-        const T dHydx = g.odx * (hy[e] - hyx);
-        const T dHxdy = g.ody * (hx[e] - hxj[e]);
-        T Ex, Ey, Ez;
-        if (lossy) {
-            Ex = ax[e] * ex[e] + (dHzdy - dHydz) * bx[e];
-            Ey = ay[e] * ey[e] + (dHxdz - dHzdx) * by[e];
-            Ez = az[e] * ez[e] + (dHydx - dHxdy) * bz[e];
-        } else {
-            Ex = ex[e] + (dHzdy - dHydz) * bx[e];
-            Ey = ey[e] + (dHxdz - dHzdx) * by[e];
-            Ez = ez[e] + (dHydx - dHxdy) * bz[e];
-        }
-        if (xw && lxs[e] >= 0) {
-            const int l = lxs[e];
-            const T kv = ld(PX.kinvE + l), bv = ld(PX.bE + l), cv = ld(PX.cE + l);
-            px2[e] = cv * dHydx + bv * px2[e];
-            px3[e] = cv * dHzdx + bv * px3[e];
-            Ez = Ez + ((px2[e] - dHydx) + dHydx * kv) * bz[e];
-            Ey = Ey - ((px3[e] - dHzdx) + dHzdx * kv) * by[e];
-        }
-        if (ly >= 0) {
-            const T kv = ld(PY.kinvE + ly), bv = ld(PY.bE + ly), cv = ld(PY.cE + ly);
-            py2[e] = cv * dHxdy + bv * py2[e];
-            py3[e] = cv * dHzdy + bv * py3[e];
-            Ez = Ez - ((py2[e] - dHxdy) + dHxdy * kv) * bz[e];
-            Ex = Ex + ((py3[e] - dHzdy) + dHzdy * kv) * bx[e];
-        }
-        if (lz >= 0) {
-            const T kv = ld(PZ.kinvE + lz), bv = ld(PZ.bE + lz), cv = ld(PZ.cE + lz);
-            pz2[e] = cv * dHxdz + bv * pz2[e];
-            pz3[e] = cv * dHydz + bv * pz3[e];
-            Ex = Ex - ((pz3[e] - dHydz) + dHydz * kv) * bx[e];
-            Ey = Ey + ((pz2[e] - dHxdz) + dHxdz * kv) * by[e];
-        }
-        if (srcb && k0 + e < g.Nx)
-            add_sources<T>(src, i, j, k0 + e, 0, T(st.z), T(st.w), Ex, Ey, Ez, true);
-        ex[e] = Ex; ey[e] = Ey; ez[e] = Ez;
-    }
-    vecb::vstore<T>(f.c[0] + p, ex); vecb::vstore<T>(f.c[1] + p, ey); vecb::vstore<T>(f.c[2] + p, ez);
-    if (ly >= 0) {
-        const int s = (i * PY.wsum + ly) * px + k0;
-        vecb::vstore<T>(PY.psi[2] + s, py2); vecb::vstore<T>(PY.psi[3] + s, py3);
-    }
-    if (lz >= 0) {
-        const int s = (lz * Ny + j) * px + k0;
-        vecb::vstore<T>(PZ.psi[2] + s, pz2); vecb::vstore<T>(PZ.psi[3] + s, pz3);
-    }
-    if (xw) {
-#pragma unroll
-        for (int e = 0; e < V; e++)
-            if (lxs[e] >= 0) {
-                const int s = (i * Ny + j) * PX.wsum + lxs[e];
-                PX.psi[2][s] = px2[e]; PX.psi[3][s] = px3[e];
+            for (int e = 0; e < V; e++) {
+                hxj[r][e] = h_min_ghost<T>(g.bc[1], hx[r][e], T(0));
+                hzj[r][e] = h_min_ghost<T>(g.bc[1], hz[r][e], T(0));
             }
+        }
+        if (i == 0 && !g.zlo) {
+#pragma unroll
+            for (int e = 0; e < V; e++) {
+                hxi[r][e] = h_min_ghost<T>(g.bc[2], hx[r][e], T(0));
+                hyi[r][e] = h_min_ghost<T>(g.bc[2], hy[r][e], T(0));
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            const T hyx = e > 0 ? hy[r][e - 1] : hy_p[r];
+            const T hzx = e > 0 ? hz[r][e - 1] : hz_p[r];
+            const T dHzdy = g.ody * (hz[r][e] - hzj[r][e]);
+            const T dHydz = g.odz * (hy[r][e] - hyi[r][e]);
+            const T dHxdz = g.odz * (hx[r][e] - hxi[r][e]);
+            const T dHzdx = g.odx * (hz[r][e] - hzx);
+            const T dHydx = g.odx * (hy[r][e] - hyx);
+            const T dHxdy = g.ody * (hx[r][e] - hxj[r][e]);
+            T Ex, Ey, Ez;
+            if (lossy) {
+                Ex = ax[r][e] * ex[r][e] + (dHzdy - dHydz) * bx[r][e];
+                Ey = ay[r][e] * ey[r][e] + (dHxdz - dHzdx) * by[r][e];
+                Ez = az[r][e] * ez[r][e] + (dHydx - dHxdy) * bz[r][e];
+            } else {
+                Ex = ex[r][e] + (dHzdy - dHydz) * bx[r][e];
+                Ey = ey[r][e] + (dHxdz - dHzdx) * by[r][e];
+                Ez = ez[r][e] + (dHydx - dHxdy) * bz[r][e];
+            }
+            if (xw && lxs[r][e] >= 0) {
+                const int l = lxs[r][e];
+                const T kv = ld(PX.kinvE + l), bv = ld(PX.bE + l), cv = ld(PX.cE + l);
+                px2[r][e] = cv * dHydx + bv * px2[r][e];
+                px3[r][e] = cv * dHzdx + bv * px3[r][e];
+                Ez = Ez + ((px2[r][e] - dHydx) + dHydx * kv) * bz[r][e];
+                Ey = Ey - ((px3[r][e] - dHzdx) + dHzdx * kv) * by[r][e];
+            }
+            if (ly[r] >= 0) {
+                const int l = ly[r];
+                const T kv = ld(PY.kinvE + l), bv = ld(PY.bE + l), cv = ld(PY.cE + l);
+                py2[r][e] = cv * dHxdy + bv * py2[r][e];
+                py3[r][e] = cv * dHzdy + bv * py3[r][e];
+                Ez = Ez - ((py2[r][e] - dHxdy) + dHxdy * kv) * bz[r][e];
+                Ex = Ex + ((py3[r][e] - dHzdy) + dHzdy * kv) * bx[r][e];
+            }
+            if (lz[r] >= 0) {
+                const int l = lz[r];
+                const T kv = ld(PZ.kinvE + l), bv = ld(PZ.bE + l), cv = ld(PZ.cE + l);
+                pz2[r][e] = cv * dHxdz + bv * pz2[r][e];
+                pz3[r][e] = cv * dHydz + bv * pz3[r][e];
+                Ex = Ex - ((pz3[r][e] - dHydz) + dHydz * kv) * bx[r][e];
+                Ey = Ey + ((pz2[r][e] - dHxdz) + dHxdz * kv) * by[r][e];
+            }
+            if (srcb && k0 + e < g.Nx)
+                add_sources<T>(src, i, j, k0 + e, 0, T(st.z), T(st.w), Ex, Ey, Ez, true);
+            ex[r][e] = Ex; ey[r][e] = Ey; ez[r][e] = Ez;
+        }
+        const int q = p[r];
+        vecb::vstore<T>(f.c[0] + q, ex[r]); vecb::vstore<T>(f.c[1] + q, ey[r]); vecb::vstore<T>(f.c[2] + q, ez[r]);
+        if (ly[r] >= 0) {
+            const int s = (i * PY.wsum + ly[r]) * px + k0;
+            vecb::vstore<T>(PY.psi[2] + s, py2[r]); vecb::vstore<T>(PY.psi[3] + s, py3[r]);
+        }
+        if (lz[r] >= 0) {
+            const int s = (lz[r] * Ny + j) * px + k0;
+            vecb::vstore<T>(PZ.psi[2] + s, pz2[r]); vecb::vstore<T>(PZ.psi[3] + s, pz3[r]);
+        }
+        if (xw) {
+#pragma unroll
+            for (int e = 0; e < V; e++)
+                if (lxs[r][e] >= 0) {
+                    const int s = (i * Ny + j) * PX.wsum + lxs[r][e];
+                    PX.psi[2][s] = px2[r][e]; PX.psi[3][s] = px3[r][e];
+                }
+        }
     }
 }
 

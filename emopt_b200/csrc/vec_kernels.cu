@@ -9,30 +9,41 @@
 #include "kernels.h"
 #include "vec_body.cuh"
 
-// Rows of a plane per block (blockDim.y, one warp per row).
+// Warps per block (blockDim.y), and rows of a plane per warp (vec_body.cuh).
 #ifndef VEC_BLOCK_ROWS
 #define VEC_BLOCK_ROWS 1
 #endif
+#ifndef VEC_WARP_ROWS32
+#define VEC_WARP_ROWS32 1
+#endif
+// float64 keeps one row per warp: two rows do not fit its register budget
+#define VEC_WARP_ROWS(T) (sizeof(T) == 4 ? VEC_WARP_ROWS32 : 1)
 
 namespace fdtdb {
 
-// Row of the warp.  With single-warp blocks it is blockIdx.y alone, which the
-// compiler knows to be the same for all lanes: the slab tests derived from it
-// become uniform branches instead of predicated code.
+// First row of the warp.  With single-warp blocks it is derived from
+// blockIdx.y alone, which the compiler knows to be the same for all lanes: the
+// slab tests derived from it become uniform branches instead of predicated
+// code.
+template <typename T>
 __device__ __forceinline__ int vec_row() {
-    return VEC_BLOCK_ROWS == 1 ? (int)blockIdx.y : (int)(blockIdx.y * VEC_BLOCK_ROWS + threadIdx.y);
+    return VEC_WARP_ROWS(T) * (VEC_BLOCK_ROWS == 1 ? (int)blockIdx.y
+                                                   : (int)(blockIdx.y * VEC_BLOCK_ROWS + threadIdx.y));
 }
 
 // Register bounds: float64 bodies are held to 18 resident single-warp CTAs
 // per SM (94-96 registers instead of 120-122: 203 instead of 210 us per step
 // on the 321 x 161 x 101 MMI block); float32 keeps its own allocation.
-#define VEC_MINB(T) (sizeof(T) == 8 ? 18 : 0)
+#ifndef VEC_MINB32
+#define VEC_MINB32 0
+#endif
+#define VEC_MINB(T) (sizeof(T) == 8 ? 18 : VEC_MINB32)
 
 template <typename T>
-__global__ void __launch_bounds__(sizeof(T) == 8 ? 32 : 256, VEC_MINB(T))
+__global__ void __launch_bounds__(sizeof(T) == 8 || VEC_MINB32 ? 32 * VEC_BLOCK_ROWS : 256, VEC_MINB(T))
 k_update_H_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off) {
-    vec_update_H<T>(g, f, src, step_base, off, blockIdx.z, vec_row(),
-                    blockIdx.x, threadIdx.x);
+    vec_update_H<T, VEC_WARP_ROWS(T)>(g, f, src, step_base, off, blockIdx.z, vec_row<T>(),
+                                      blockIdx.x, threadIdx.x);
 }
 
 // The E kernel is bounded by its real block size: that keeps it at 64
@@ -40,8 +51,8 @@ k_update_H_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* s
 template <typename T>
 __global__ void __launch_bounds__(32 * VEC_BLOCK_ROWS, VEC_MINB(T))
 k_update_E_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off) {
-    vec_update_E<T>(g, f, src, step_base, off, blockIdx.z, vec_row(),
-                    blockIdx.x, threadIdx.x);
+    vec_update_E<T, VEC_WARP_ROWS(T)>(g, f, src, step_base, off, blockIdx.z, vec_row<T>(),
+                                      blockIdx.x, threadIdx.x);
 }
 
 template <typename T>
@@ -52,7 +63,8 @@ cudaError_t launch_step_vec(const GridView<T>& g, T* const* fields, const Source
     for (int c = 0; c < 6; c++) f.c[c] = fields[c];
     const int nvec = (g.Nx + V - 1) / V;
     dim3 block(32, VEC_BLOCK_ROWS);
-    dim3 grid((nvec + 31) / 32, (g.Ny + VEC_BLOCK_ROWS - 1) / VEC_BLOCK_ROWS, g.Nz);
+    const int rows = VEC_BLOCK_ROWS * VEC_WARP_ROWS(T);
+    dim3 grid((nvec + 31) / 32, (g.Ny + rows - 1) / rows, g.Nz);
     k_update_H_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
     k_update_E_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
     return cudaGetLastError();
@@ -66,7 +78,8 @@ cudaError_t launch_half_vec(const GridView<T>& g, T* const* fields, const Source
     for (int c = 0; c < 6; c++) f.c[c] = fields[c];
     const int nvec = (g.Nx + V - 1) / V;
     dim3 block(32, VEC_BLOCK_ROWS);
-    dim3 grid((nvec + 31) / 32, (g.Ny + VEC_BLOCK_ROWS - 1) / VEC_BLOCK_ROWS, g.Nz);
+    const int rows = VEC_BLOCK_ROWS * VEC_WARP_ROWS(T);
+    dim3 grid((nvec + 31) / 32, (g.Ny + rows - 1) / rows, g.Nz);
     if (half == 0) k_update_H_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
     else k_update_E_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
     return cudaGetLastError();
