@@ -351,12 +351,13 @@ using fdtdb::c128;
 extern "C" int FDTD_interp_field(int device, void* stream, int comp, const fdtd_complex128* raw,
                                  const int* geom, fdtd_complex128* out, char* msg, int msglen) {
     fdtdb::Geom g;
-    if (comp < 0 || comp > 5 || !raw || !out || !geom || !fdtdb::geom_from(geom, &g))
-        return fdtdb::fail(msg, msglen, FDTD_ERR_ARG, "FDTD_interp_field: invalid component, pointer or geometry");
+    if (comp < 0 || comp > 5 || !geom || !fdtdb::geom_from(geom, &g))
+        return fdtdb::fail(msg, msglen, FDTD_ERR_ARG, "FDTD_interp_field: invalid component or geometry");
+    const long long n = (long long)g.oi * g.oj * g.ok;
+    if (n == 0) return FDTD_OK;   // an empty domain (null pointers allowed)
+    if (!raw || !out) return fdtdb::fail(msg, msglen, FDTD_ERR_ARG, "FDTD_interp_field: null array");
     fdtdb::DeviceScope ds(device);
     if (ds.err != cudaSuccess) return fdtdb::fail(msg, msglen, FDTD_ERR_CUDA, "FDTD_interp_field: %s", cudaGetErrorString(ds.err));
-    const long long n = (long long)g.oi * g.oj * g.ok;
-    if (n == 0) return FDTD_OK;
     cudaStream_t st = (cudaStream_t)stream;
     cudaGetLastError();
     fdtdb::k_interp<<<fdtdb::blocks_for_n(n), 256, 0, st>>>(reinterpret_cast<const c128*>(raw), g, comp,
@@ -369,12 +370,15 @@ extern "C" int FDTD_interp_field(int device, void* stream, int comp, const fdtd_
 extern "C" int FDTD_interp_field_T(int device, void* stream, int comp, const fdtd_complex128* gout,
                                    const int* geom, fdtd_complex128* graw, char* msg, int msglen) {
     fdtdb::Geom g;
-    if (comp < 0 || comp > 5 || !gout || !graw || !geom || !fdtdb::geom_from(geom, &g))
-        return fdtdb::fail(msg, msglen, FDTD_ERR_ARG, "FDTD_interp_field_T: invalid component, pointer or geometry");
+    if (comp < 0 || comp > 5 || !geom || !fdtdb::geom_from(geom, &g))
+        return fdtdb::fail(msg, msglen, FDTD_ERR_ARG, "FDTD_interp_field_T: invalid component or geometry");
+    const long long n = (long long)g.ni * g.nj * g.nk;
+    if (n == 0) return FDTD_OK;   // an empty block (null pointers allowed)
+    // an empty output: the block's cotangent is zero (the kernel reads no gout)
+    if (!graw || (!gout && (long long)g.oi * g.oj * g.ok > 0))
+        return fdtdb::fail(msg, msglen, FDTD_ERR_ARG, "FDTD_interp_field_T: null array");
     fdtdb::DeviceScope ds(device);
     if (ds.err != cudaSuccess) return fdtdb::fail(msg, msglen, FDTD_ERR_CUDA, "FDTD_interp_field_T: %s", cudaGetErrorString(ds.err));
-    const long long n = (long long)g.ni * g.nj * g.nk;
-    if (n == 0) return FDTD_OK;
     cudaStream_t st = (cudaStream_t)stream;
     cudaGetLastError();
     fdtdb::k_interp_T<<<fdtdb::blocks_for_n(n), 256, 0, st>>>(reinterpret_cast<const c128*>(gout), g, comp,
@@ -387,8 +391,8 @@ extern "C" int FDTD_interp_field_T(int device, void* stream, int comp, const fdt
 extern "C" int FDTD_dfdx_interp(int device, void* stream, int comp, const fdtd_complex128* dF, int nx,
                                 int ny, int nz, int qx, int qy, fdtd_complex128* out, char* msg,
                                 int msglen) {
-    if (comp < 0 || comp > 5 || !dF || !out || nx < 0 || ny < 0 || nz < 0 || qx < 0 || qx > 2 ||
-        qy < -1 || qy > 1)
+    if (comp < 0 || comp > 5 || !out || nx < 0 || ny < 0 || nz < 0 || qx < 0 || qx > 2 ||
+        qy < -1 || qy > 1 || (!dF && (long long)nx * ny * nz > 0))
         return fdtdb::fail(msg, msglen, FDTD_ERR_ARG, "FDTD_dfdx_interp: invalid argument");
     fdtdb::DeviceScope ds(device);
     if (ds.err != cudaSuccess) return fdtdb::fail(msg, msglen, FDTD_ERR_CUDA, "FDTD_dfdx_interp: %s", cudaGetErrorString(ds.err));

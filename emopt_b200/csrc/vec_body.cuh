@@ -63,15 +63,13 @@ __device__ __forceinline__ void vstore(T* p, const T (&d)[V16<T>::N]) {
     *reinterpret_cast<typename V16<T>::type*>(p) = v;
 }
 
-// L2 prefetch distance in planes (0: none).  The warp that updates row j of
-// plane i asks L2 for the same 64-cell segment of plane i + VEC_PREFETCH of
+// L2 prefetch (GridView::pf planes ahead, 0: none).  The warp that updates
+// row j of plane i asks L2 for the same 64-cell segment of plane i + pf of
 // the arrays it streams, so that the warp which later updates that plane
 // finds them in L2 (fp32 MMI block: 119.4 instead of 121.0 us per step at
 // distance 2, fp64 199 instead of 205; distance 4 and 8 and one bulk request
-// per array gained less).
-#ifndef VEC_PREFETCH
-#define VEC_PREFETCH 2
-#endif
+// per array gained less).  The host enables it only when the prefetched
+// planes fit in L2 beside the planes being updated (make_view).
 
 // p: first cell of the warp's segment; `room` cells of the row's pitch remain
 // from there, so no request leaves the row.
@@ -180,11 +178,11 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
 
-    if (VEC_PREFETCH > 0 && i + VEC_PREFETCH < Nz && xb * 32 * V < g.Nx) {
+    if (g.pf > 0 && i + g.pf < Nz && xb * 32 * V < g.Nx) {
 #pragma unroll
         for (int r = 0; r < NR; r++)
             if (j0 + r < Ny) {
-                const long long q = (long long)(i + VEC_PREFETCH) * g.plane + (long long)(j0 + r) * px + xb * 32 * V;
+                const long long q = (long long)(i + g.pf) * g.plane + (long long)(j0 + r) * px + xb * 32 * V;
 #pragma unroll
                 for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
             }
@@ -370,11 +368,11 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
     const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
     const bool lossy = g.aE[0] != nullptr;
 
-    if (VEC_PREFETCH > 0 && i + VEC_PREFETCH < g.Nz && xb * 32 * V < g.Nx) {
+    if (g.pf > 0 && i + g.pf < g.Nz && xb * 32 * V < g.Nx) {
 #pragma unroll
         for (int r = 0; r < NR; r++)
             if (j0 + r < Ny) {
-                const long long q = (long long)(i + VEC_PREFETCH) * g.plane + (long long)(j0 + r) * px + xb * 32 * V;
+                const long long q = (long long)(i + g.pf) * g.plane + (long long)(j0 + r) * px + xb * 32 * V;
 #pragma unroll
                 for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
 #pragma unroll
