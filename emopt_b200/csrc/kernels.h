@@ -18,11 +18,13 @@ template <typename T>
 cudaError_t launch_step_vec(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
                             const long long* step_base, int off, cudaStream_t st);
 
-// One half step (half 0: H, 1: E) of the vector pair: the z slabs of a
-// distributed solve exchange halo planes between the two.
+// One half step (half 0: H, 1: E) of the vector pair over planes
+// [i0, i0 + ni): the z slabs of a distributed solve exchange halo planes
+// between the two, and update the planes next to a halo apart from the rest.
 template <typename T>
 cudaError_t launch_half_vec(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
-                            const long long* step_base, int off, int half, cudaStream_t st);
+                            const long long* step_base, int off, int half, int i0, int ni,
+                            cudaStream_t st);
 
 // One fused time step (zmarch_kernels.cu): H and E of every cell, reading the
 // fields and CPML state of (ga, fa) and writing those of (gb, fb); each

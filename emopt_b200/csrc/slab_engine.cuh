@@ -12,6 +12,14 @@
 //     for each step n:  [E halo from the slab above]  FDTD_slab_step(n, 0)
 //                       [H halo from the slab below]  FDTD_slab_step(n, 1)
 //
+// or, overlapping each exchange with the planes that do not need it
+// (FDTD_slab_step_part: part 1 = the planes that read no halo, part 2 = the
+// plane next to the halo):
+//
+//     step(n, 0, part 1); [wait for the E halo] step(n, 0, part 2);
+//     [start the H exchange] step(n, 1, part 1); [wait for the H halo]
+//     step(n, 1, part 2); [start the E exchange]
+//
 // The field arrays carry one halo plane below and above the slab; the
 // exchange writes into them (FDTD_slab_halo gives the device addresses).  The
 // vector kernels read a halo plane where the slab has a neighbour and apply
@@ -104,14 +112,30 @@ int slab_begin_impl(FDTDHandle* h, const FDTDSolveOptions* o, const long long* c
     return h->sync_check("FDTD_slab_begin");
 }
 
+// Planes of half step `half` for part 0 (all), 1 (the planes that read no
+// halo plane) or 2 (the plane next to a neighbour's halo: the top plane of the
+// H update reads E above, the bottom plane of the E update reads H below).
+void slab_planes(const FDTDHandle* h, int half, int part, int* i0, int* ni) {
+    const int I = h->Nz;
+    const bool edge = half == 0 ? h->slab_hi != 0 : h->slab_lo != 0;
+    const int eplane = half == 0 ? I - 1 : 0;
+    if (part == 0 || (!edge && part == 1)) { *i0 = 0; *ni = I; return; }
+    if (!edge) { *i0 = 0; *ni = 0; return; }                // part 2 without a neighbour
+    if (part == 2) { *i0 = eplane; *ni = 1; return; }
+    *i0 = half == 0 ? 0 : 1;                                // part 1 with a neighbour
+    *ni = I - 1;
+}
+
 template <typename T>
-int slab_step_impl(FDTDHandle* h, long long n, int half) {
+int slab_step_impl(FDTDHandle* h, long long n, int half, int part) {
     Resident<T>& r = resident<T>(h);
     T* f[6];
     slab_fields<T>(r, f);
     fdtdb::GridView<T> g = slab_view<T>(h, r);
+    int i0, ni;
+    slab_planes(h, half, part, &i0, &ni);
     CK(fdtdb::launch_half_vec<T>(g, f, slab_src<T>(h), dptr<long long>(r.stepbase), (int)n, half,
-                                 h->stream));
+                                 i0, ni, h->stream));
     return FDTD_OK;
 }
 
@@ -258,9 +282,15 @@ extern "C" int FDTD_slab_begin(FDTDHandle* h, const FDTDSolveOptions* o, const l
 }
 
 extern "C" int FDTD_slab_step(FDTDHandle* h, long long n, int half) {
-    if (!slab_ready(h) || (half != 0 && half != 1) || n < 0 || n >= (1LL << 31))
-        return h ? h->fail(FDTD_ERR_ARG, "FDTD_slab_step: no slab begun, or bad step") : FDTD_ERR_ARG;
-    return h->precision == 32 ? slab_step_impl<float>(h, n, half) : slab_step_impl<double>(h, n, half);
+    return FDTD_slab_step_part(h, n, half, 0);
+}
+
+extern "C" int FDTD_slab_step_part(FDTDHandle* h, long long n, int half, int part) {
+    if (!slab_ready(h) || (half != 0 && half != 1) || n < 0 || n >= (1LL << 31) || part < 0 || part > 2)
+        return h ? h->fail(FDTD_ERR_ARG, "FDTD_slab_step_part: no slab begun, or bad step or part")
+                 : FDTD_ERR_ARG;
+    return h->precision == 32 ? slab_step_impl<float>(h, n, half, part)
+                              : slab_step_impl<double>(h, n, half, part);
 }
 
 extern "C" int FDTD_slab_halo(FDTDHandle* h, void** ptrs, long long* plane_elems) {

@@ -41,8 +41,9 @@ __device__ __forceinline__ int vec_row() {
 
 template <typename T>
 __global__ void __launch_bounds__(sizeof(T) == 8 || VEC_MINB32 ? 32 * VEC_BLOCK_ROWS : 256, VEC_MINB(T))
-k_update_H_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off) {
-    vec_update_H<T, VEC_WARP_ROWS(T)>(g, f, src, step_base, off, blockIdx.z, vec_row<T>(),
+k_update_H_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
+               int i0) {
+    vec_update_H<T, VEC_WARP_ROWS(T)>(g, f, src, step_base, off, i0 + (int)blockIdx.z, vec_row<T>(),
                                       blockIdx.x, threadIdx.x);
 }
 
@@ -50,8 +51,9 @@ k_update_H_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* s
 // registers in float32 (80 under the 256-thread bound), ~4% faster per step.
 template <typename T>
 __global__ void __launch_bounds__(32 * VEC_BLOCK_ROWS, VEC_MINB(T))
-k_update_E_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off) {
-    vec_update_E<T, VEC_WARP_ROWS(T)>(g, f, src, step_base, off, blockIdx.z, vec_row<T>(),
+k_update_E_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
+               int i0) {
+    vec_update_E<T, VEC_WARP_ROWS(T)>(g, f, src, step_base, off, i0 + (int)blockIdx.z, vec_row<T>(),
                                       blockIdx.x, threadIdx.x);
 }
 
@@ -65,32 +67,34 @@ cudaError_t launch_step_vec(const GridView<T>& g, T* const* fields, const Source
     dim3 block(32, VEC_BLOCK_ROWS);
     const int rows = VEC_BLOCK_ROWS * VEC_WARP_ROWS(T);
     dim3 grid((nvec + 31) / 32, (g.Ny + rows - 1) / rows, g.Nz);
-    k_update_H_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
-    k_update_E_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
+    k_update_H_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off, 0);
+    k_update_E_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off, 0);
     return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_half_vec(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
-                            const long long* step_base, int off, int half, cudaStream_t st) {
+                            const long long* step_base, int off, int half, int i0, int ni,
+                            cudaStream_t st) {
     constexpr int V = vecb::V16<T>::N;
+    if (ni <= 0) return cudaSuccess;
     Fields<T> f;
     for (int c = 0; c < 6; c++) f.c[c] = fields[c];
     const int nvec = (g.Nx + V - 1) / V;
     dim3 block(32, VEC_BLOCK_ROWS);
     const int rows = VEC_BLOCK_ROWS * VEC_WARP_ROWS(T);
-    dim3 grid((nvec + 31) / 32, (g.Ny + rows - 1) / rows, g.Nz);
-    if (half == 0) k_update_H_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
-    else k_update_E_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off);
+    dim3 grid((nvec + 31) / 32, (g.Ny + rows - 1) / rows, ni);
+    if (half == 0) k_update_H_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off, i0);
+    else k_update_E_vec<T><<<grid, block, 0, st>>>(g, f, src, step_base, off, i0);
     return cudaGetLastError();
 }
 
 template cudaError_t launch_half_vec<float>(const GridView<float>&, float* const*,
                                             const SourceList<float>&, const long long*, int, int,
-                                            cudaStream_t);
+                                            int, int, cudaStream_t);
 template cudaError_t launch_half_vec<double>(const GridView<double>&, double* const*,
                                              const SourceList<double>&, const long long*, int, int,
-                                             cudaStream_t);
+                                             int, int, cudaStream_t);
 template cudaError_t launch_step_vec<float>(const GridView<float>&, float* const*,
                                             const SourceList<float>&, const long long*, int,
                                             cudaStream_t);

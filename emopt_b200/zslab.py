@@ -198,6 +198,11 @@ class CudaSlab:
     def half_step(self, n: int, half: int):
         self._ok(libFDTD.FDTD_slab_step(self.h, n, half), "FDTD_slab_step")
 
+    def half_step_part(self, n: int, half: int, part: int):
+        """Part 1: the planes that read no halo plane; part 2: the plane next to
+        the neighbour's halo (FDTD_slab_step_part)."""
+        self._ok(libFDTD.FDTD_slab_step_part(self.h, n, half, part), "FDTD_slab_step_part")
+
     def sample(self):
         sp = ctypes.c_void_p()
         self._ok(libFDTD.FDTD_slab_sample(self.h, ctypes.byref(sp)), "FDTD_slab_sample")
@@ -227,18 +232,34 @@ class CudaSlab:
 class LocalLink:
     """Slabs of one process: halo planes and probe sums move by device copies."""
 
+    # the copies run in stream order on the device: splitting the half steps
+    # to overlap them would only add launches
+    overlap = False
+
     def __init__(self, slabs):
         self.slabs = slabs
 
-    def exchange_E(self):
+    def start_E(self):
         for lo, hi in zip(self.slabs[:-1], self.slabs[1:]):
             for c in range(2):
                 lo.halo["E_recv"][c].copy_(hi.halo["E_send"][c])
 
-    def exchange_H(self):
+    def start_H(self):
         for lo, hi in zip(self.slabs[:-1], self.slabs[1:]):
             for c in range(2):
                 hi.halo["H_recv"][c].copy_(lo.halo["H_send"][c])
+
+    def wait_E(self):
+        """The copies run in stream order: nothing to wait for."""
+
+    def wait_H(self):
+        """The copies run in stream order: nothing to wait for."""
+
+    def exchange_E(self):
+        self.start_E()
+
+    def exchange_H(self):
+        self.start_H()
 
     def sum_samples(self, tensors):
         total = tensors[0].clone()
@@ -252,6 +273,10 @@ class TorchLink:
     """One slab per process; neighbours are ranks - 1 and + 1 of the default
     ``torch.distributed`` group (NCCL on GPUs, gloo on CPU tensors)."""
 
+    # transfers between processes run beside the kernels: overlap them with
+    # the planes that do not need the halo
+    overlap = True
+
     def __init__(self, slab):
         import torch.distributed as dist
         self.dist = dist
@@ -259,26 +284,48 @@ class TorchLink:
         self.rank = dist.get_rank()
         self.size = dist.get_world_size()
 
+        self._pending = {"E": [], "H": []}
+
     def _swap(self, send, send_to, recv, recv_from):
+        """Start the point-to-point operations; returns their works."""
         dist = self.dist
         ops = []
         if recv_from is not None:
             ops += [dist.P2POp(dist.irecv, t, recv_from) for t in recv]
         if send_to is not None:
             ops += [dist.P2POp(dist.isend, t, send_to) for t in send]
-        if ops:
-            for w in dist.batch_isend_irecv(ops):
-                w.wait()
+        return dist.batch_isend_irecv(ops) if ops else []
+
+    def start_E(self):
+        s = self.slabs[0]
+        self._pending["E"] = self._swap(s.halo["E_send"], self.rank - 1 if s.has_lo else None,
+                                        s.halo["E_recv"], self.rank + 1 if s.has_hi else None)
+
+    def start_H(self):
+        s = self.slabs[0]
+        self._pending["H"] = self._swap(s.halo["H_send"], self.rank + 1 if s.has_hi else None,
+                                        s.halo["H_recv"], self.rank - 1 if s.has_lo else None)
+
+    def _wait(self, which):
+        # on CUDA tensors the wait orders the current stream after the
+        # transfer (the host does not block); on CPU tensors it blocks
+        for w in self._pending[which]:
+            w.wait()
+        self._pending[which] = []
+
+    def wait_E(self):
+        self._wait("E")
+
+    def wait_H(self):
+        self._wait("H")
 
     def exchange_E(self):
-        s = self.slabs[0]
-        self._swap(s.halo["E_send"], self.rank - 1 if s.has_lo else None,
-                   s.halo["E_recv"], self.rank + 1 if s.has_hi else None)
+        self.start_E()
+        self.wait_E()
 
     def exchange_H(self):
-        s = self.slabs[0]
-        self._swap(s.halo["H_send"], self.rank + 1 if s.has_hi else None,
-                   s.halo["H_recv"], self.rank - 1 if s.has_lo else None)
+        self.start_H()
+        self.wait_H()
 
     def sum_samples(self, tensors):
         for t in tensors:
@@ -303,7 +350,7 @@ def run(slabs, link, Tn: int, rtol: float, Nmax: float, fixed_steps: int | None 
     fixed = bool(fixed_steps)
     last = fixed_steps - 1 if fixed else int(np.floor(Nmax))
 
-    def steps(n, count):
+    def steps_plain(n, count):
         for m in range(n, n + count):
             link.exchange_E()
             for s in slabs:
@@ -311,6 +358,33 @@ def run(slabs, link, Tn: int, rtol: float, Nmax: float, fixed_steps: int | None 
             link.exchange_H()
             for s in slabs:
                 s.half_step(m, 1)
+
+    def steps_overlapped(n, count):
+        # Each exchange overlaps the planes that do not need it: the H update
+        # of every plane but the top one runs while the E halo from above is in
+        # flight, then the top plane; the H halo goes up while the E update of
+        # every plane but the bottom one runs, then the bottom plane; the E
+        # halo leaves at the end of the step (the fields it carries do not
+        # change before the next step's H update reads them).
+        if count <= 0:
+            return
+        link.start_E()
+        for m in range(n, n + count):
+            for s in slabs:
+                s.half_step_part(m, 0, 1)
+            link.wait_E()
+            for s in slabs:
+                s.half_step_part(m, 0, 2)
+            link.start_H()
+            for s in slabs:
+                s.half_step_part(m, 1, 1)
+            link.wait_H()
+            for s in slabs:
+                s.half_step_part(m, 1, 2)
+            if m + 1 < n + count:
+                link.start_E()
+
+    steps = steps_overlapped if getattr(link, "overlap", False) else steps_plain
 
     def probe(n_last):
         link.sum_samples([s.sample() for s in slabs])

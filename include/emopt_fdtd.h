@@ -269,6 +269,14 @@ int FDTD_slab_begin(FDTDHandle *h, const FDTDSolveOptions *o, const long long *c
 /* Half step of time step n: half 0 updates H, half 1 updates E. */
 int FDTD_slab_step(FDTDHandle *h, long long n, int half);
 
+/* Part of a half step, so that an exchange overlaps the planes that do not
+ * need it: part 1 = every plane that reads no halo plane (all of them when
+ * the slab has no neighbour on that side), part 2 = the plane next to the
+ * neighbour's halo (the top plane of the H update, the bottom plane of the E
+ * update; nothing without a neighbour), part 0 = all planes.  Parts 1 and 2
+ * together equal part 0. */
+int FDTD_slab_step_part(FDTDHandle *h, long long n, int half, int part);
+
 /* Device addresses of the exchanged planes (plane_elems elements each, in the
  * slab's precision): ptrs[0..1] Ex, Ey of plane 0 (send down); ptrs[2..3] the
  * Ex, Ey halo above (receive from the slab above); ptrs[4..5] Hx, Hy of the

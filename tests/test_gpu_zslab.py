@@ -38,9 +38,27 @@ def _single(p, precision):
     return np.stack([sim._raw(c, False) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")]), info
 
 
-def _slabs(p, nslab, precision):
+class OverlapLocalLink(zslab.LocalLink):
+    """Device copies with the overlapped schedule of the NCCL transport: every
+    half step in two parts (the planes that read no halo, then the plane next
+    to it, FDTD_slab_step_part) around the exchange."""
+    overlap = True
+
+
+def _slabs(p, nslab, precision, overlap=False):
     ranges = zslab.ownership(p.shape[0], nslab)
-    res, parts = zslab.solve(p, ranges, precision=precision)
+    link = None
+    if overlap:
+        ss = zslab.SlabSet(p, ranges, precision=precision)
+        try:
+            ss.begin()
+            ss.link = OverlapLocalLink(ss.slabs)
+            res = ss.run()
+            parts = ss.finish()
+        finally:
+            ss.close()
+    else:
+        res, parts = zslab.solve(p, ranges, precision=precision, link=link)
     F = np.stack([np.concatenate([parts[s][c] for s in range(len(ranges))]) for c in range(6)])
     return F, res
 
@@ -52,6 +70,19 @@ def test_fixed_steps_equal_single_gpu_solve(name, precision):
     p = P.random_box(**dict(kw, fixed_steps=150))
     F1, info = _single(p, precision)
     F, res = _slabs(p, nslab, precision)
+    assert res.steps == info["steps"] and res.n_main == info["n_main"]
+    assert np.array_equal(F, F1)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name", list(CASES))
+def test_overlapped_schedule_equals_single_gpu_solve(name, precision):
+    """The split half steps of the overlapped loop give the same fields, bit
+    for bit, as the whole-grid solve."""
+    kw, nslab = CASES[name]
+    p = P.random_box(**dict(kw, fixed_steps=150))
+    F1, info = _single(p, precision)
+    F, res = _slabs(p, nslab, precision, overlap=True)
     assert res.steps == info["steps"] and res.n_main == info["n_main"]
     assert np.array_equal(F, F1)
 
