@@ -55,6 +55,12 @@ def parse_args():
                     choices=["mmi", "waveguide", "serving", "grad", "grating", "zslab", "modes"])
     ap.add_argument("--slabs", type=int, default=2,
                     help="zslab on one process: z slabs on this GPU (under torchrun: one per rank)")
+    ap.add_argument("--copy-halo", action="store_true",
+                    help="zslab on one process: exchange halo planes by device copies instead of "
+                         "reading the neighbouring slabs' planes in place")
+    ap.add_argument("--overlap", action="store_true",
+                    help="zslab on one process: halo copies on a side stream, half steps split around "
+                         "them (the schedule of the NCCL transport)")
     ap.add_argument("--requests", type=int, default=512, help="serving: requests in the stream")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: mean arrivals per second")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
@@ -583,7 +589,8 @@ def run_zslab(args):
     ranges = zslab.ownership(p.shape[0], nslab)
     torch.cuda.set_device(local)
     ss = zslab.SlabSet(p, ranges, precision=args.precision, devices=[local],
-                       rank=rank if world > 1 else None)
+                       rank=rank if world > 1 else None, overlap=args.overlap,
+                       direct=False if args.copy_halo else None)
     times, res = [], None
     with ClockSampler(local) as clk:
         for it in range(args.warmup + args.steps):
@@ -610,7 +617,9 @@ def run_zslab(args):
         "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
         "config": {"workload": "mmi_321x161x101_zslab", "slabs": nslab, "ranges": ranges,
                    "time_steps_per_solve": res.steps, "n_main": res.n_main,
-                   "transport": "nccl" if world > 1 else "device copies (one GPU)"},
+                   "transport": "nccl" if world > 1 else
+                   ("neighbour planes read in place (one GPU)" if ss.direct else "device copies (one GPU)"),
+                   "schedule": "overlapped" if world > 1 or args.overlap else "plain"},
         "step_us": 1e6 * t / res.steps,
         "clocks": clk.summary(),
     }

@@ -141,6 +141,7 @@ struct FDTDHandle {
     int slab = 0;
     int slab_i0 = 0, slab_Nz = 0, slab_lo = 0, slab_hi = 0;
     int slab_np = 0;                 // probe points of all slabs
+    const void* slab_zhalo[4] = {nullptr, nullptr, nullptr, nullptr};   // FDTD_slab_set_halo_source
     long long slab_Tn = 0;
     fdtdb::SourceList<float> slab_src32;
     fdtdb::SourceList<double> slab_src64;
@@ -956,6 +957,7 @@ fdtdb::GridView<T> make_view(FDTDHandle* h, Resident<T>& r, int set = 0) {
         P.bE = dptr<T>(r.tab[a][4]); P.cE = dptr<T>(r.tab[a][5]);
     }
     g.zlo = g.zhi = 0;
+    for (int c = 0; c < 4; c++) g.zhalo[c] = nullptr;
     g.chk = nullptr;
     // prefetch two planes ahead when four planes of the nine streamed arrays
     // (the two being updated and the two prefetched) take at most half of L2

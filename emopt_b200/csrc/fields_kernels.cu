@@ -241,9 +241,9 @@ __global__ void k_dfdx_interp(const c128* dF, int nz, int ny, int nx, int comp, 
 }
 
 // Source power: per plane p, the sum over its cells of
-// Re(E1 conj(H2) - E2 conj(H1)) with (E1, H2, E2, H1) = (Ey, Hz, Ez, Hy) for
-// a plane normal to x, (Ex, Hz, Ez, Hx) for y, (Ex, Hy, Ey, Hx) for z, every
-// component interpolated as above.  One CTA sums a stretch of cells (warp
+// Re(E1 conj(H2) - E2 conj(H1)) = Re(E x H*) . n with (E1, H2, E2, H1) =
+// (Ey, Hz, Ez, Hy) for a plane normal to x, (Ez, Hx, Ex, Hz) for y, (Ex, Hy,
+// Ey, Hx) for z (kFluxComps), every component interpolated as above.  One CTA sums a stretch of cells (warp
 // shuffles, then shared memory, in a fixed order) into partial[p][block];
 // k_sum_partials adds the partials of each plane in order.
 struct PlaneSet {
@@ -254,6 +254,9 @@ struct PlaneSet {
 };
 
 constexpr int kPowThreads = 256;
+
+// (E1, H2, E2, H1) of the flux through a plane normal to x, y, z
+__constant__ int kFluxComps[3][4] = {{1, 5, 2, 4}, {2, 3, 0, 5}, {0, 4, 1, 3}};
 
 __device__ __forceinline__ double block_sum(double v) {
     __shared__ double red[kPowThreads / 32];
@@ -271,7 +274,7 @@ __global__ void __launch_bounds__(kPowThreads) k_power_partials(PlaneSet ps, dou
     const int p = blockIdx.y;
     const Geom& g = ps.g[p];
     const int ax = ps.axis[p];
-    const int c1 = ax == 0 ? 1 : 0, c2 = ax == 2 ? 4 : 5, c3 = ax == 2 ? 1 : 2, c4 = ax == 0 ? 4 : 3;
+    const int c1 = kFluxComps[ax][0], c2 = kFluxComps[ax][1], c3 = kFluxComps[ax][2], c4 = kFluxComps[ax][3];
     const long long n = (long long)g.oi * g.oj * g.ok;
     double acc = 0;
     for (long long q = blockIdx.x * (long long)kPowThreads + threadIdx.x; q < n;

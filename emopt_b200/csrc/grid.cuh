@@ -71,11 +71,36 @@ struct GridView {
     // Nz - 1 (zhi): the field arrays then have a halo plane there, filled by
     // the exchange, which is read instead of applying the boundary rule
     char zlo, zhi;
+    // where those neighbour planes are read (zlo / zhi set): Ex, Ey of the
+    // plane above (zhalo[0], [1]) and Hx, Hy of the plane below ([2], [3]),
+    // each Ny x px with the rows of a plane -- the slab's own halo planes, or
+    // the neighbouring slab's boundary planes when it lives on this device
+    const T* zhalo[4];
     int* chk;                      // builds with FDTD_BOUNDS_CHECK: first failed index check (else unused)
     int pf;                        // L2 prefetch distance in planes of the vector bodies (0: none)
     PmlAxis<T> pml[3];
     const double4* step_tab;       // per step: (S_H, C_H, S_E, C_E)
 };
+
+// Loop state of one request in the batched stepping (serve_kernels.cu).
+enum ServeState { SERVE_FREE = 0, SERVE_RUN = 1, SERVE_TAIL = 2, SERVE_EXTRACT = 3, SERVE_DONE = 4 };
+
+// What a half step of one served request reads besides its grid: the
+// request's loop state and capture flag (device memory, written by the
+// events kernel between steps) and its two snapshot sets.  The half step
+// stores only while the state is RUN, TAIL or EXTRACT; with capture = 1 or 2
+// the H half step also writes the six fields it read (the state after the
+// previous step) into snap[capture - 1].
+template <typename T>
+struct ServeGate {
+    const int* state;
+    const int* capture;
+    T* snap[2][6];
+};
+
+__device__ __forceinline__ bool serve_running(int state) {
+    return state == SERVE_RUN || state == SERVE_TAIL || state == SERVE_EXTRACT;
+}
 
 // Local CPML slab index of coordinate c on axis a, or -1.
 template <typename T>

@@ -94,9 +94,8 @@ struct ProbeDev {
 };
 
 // ---------------------------------------------------------------- serving
-// Loop state of one request in the batched stepping (serve_kernels.cu).
-enum ServeState { SERVE_FREE = 0, SERVE_RUN = 1, SERVE_TAIL = 2, SERVE_EXTRACT = 3, SERVE_DONE = 4 };
-
+// Control block of one served request (device memory): its step counter and
+// the state of its loop (ServeState, grid.cuh).
 struct ServeCtl {
     long long n;            // time steps taken
     long long Tn, last, n0, nprobes;
@@ -115,17 +114,12 @@ struct ServeView {
     long long nxb;          // 32-vector blocks per row
 };
 
-// Resident single-warp CTAs per SM of the batched step kernels.
+// One time step of one served request: its H and E half steps (grid and
+// fields in the kernel parameters, as the single-solve kernels) and its loop
+// events (step counter, probes, captures, end).  Fixed launch shapes while
+// the request is admitted (graph-capturable).
 template <typename T>
-int serve_step_ctas_per_sm();
-
-// One time step of every request in the slot tables: H, E, loop events,
-// captures.  Fixed launch shapes (graph-capturable); cap_count is one int of
-// device memory for the per-step capture count.
-template <typename T>
-cudaError_t launch_serve_step(const ServeView<T>* views, ServeCtl* ctl, const long long* task0,
-                              int nslots, long long step_ctas, int copy_ctas, int* cap_count,
-                              cudaStream_t st);
+cudaError_t launch_serve_request_step(const ServeView<T>& v, ServeCtl* ctl, cudaStream_t st);
 
 template <typename T>
 void launch_probe(const T* Ex, const T* Ey, const T* Ez, ProbeDev pd, long long* step_base,

@@ -7,9 +7,11 @@
 //
 // A request is a configured handle plus its solve options.  Admission checks
 // the engine's device-memory budget and a free slot, allocates and prepares
-// the request's resident state, and enters it into the device slot tables;
-// from then on the request advances with every graph replay
-// (FDTD_serve_advance), together with all other active requests.  A request
+// the request's resident state, and enters it into the slot tables; from the
+// next graph replay on (FDTD_serve_advance) the request advances with all
+// other active requests: the graph holds one branch per admitted request
+// (L time steps of its own launches, serve_kernels.cu) and is captured again
+// at the first replay after the set of requests changed.  A request
 // whose loop ended (converged, step budget or fixed length) stops stepping on
 // its own; FDTD_serve_collect extracts its complex fields into the handle's t0
 // arrays, fills its result and frees its memory.  Admission and collection
@@ -19,19 +21,19 @@ struct FDTDServe {
     int device = 0;
     cudaStream_t stream = nullptr;
     double budget = 0, used = 0;
-    int cap = 0, L = 0, step_ctas = 0, copy_ctas = 0;
-    fdtdb::ServeView<float>* d_views = nullptr;
+    int cap = 0, L = 0;
     fdtdb::ServeCtl* d_ctl = nullptr;
-    long long* d_task0 = nullptr;
-    int* d_cap = nullptr;                      // per-step capture count
     fdtdb::ServeCtl* h_ctl = nullptr;          // pinned mirror
     std::vector<fdtdb::ServeView<float>> views;
-    std::vector<long long> task0;
     std::vector<FDTDHandle*> slot_h;
     std::vector<double> slot_bytes;
     std::vector<long long> admitted_step;      // replay count at admission
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
+    bool dirty = true;                         // the graph does not hold the current requests
+    std::vector<cudaStream_t> aux;             // capture streams of the branches
+    std::vector<cudaEvent_t> join;
+    cudaEvent_t fork = nullptr;
     long long replays = 0;
     int status = FDTD_OK;
     std::string message;
@@ -86,34 +88,52 @@ double resident_bytes(const Resident<T>& r) {
     return b;
 }
 
-int serve_upload_tables(FDTDServe* s) {
-    long long acc = 0;
-    for (int q = 0; q < s->cap; q++) {
-        s->task0[q] = acc;
-        if (s->slot_h[q]) {
-            const auto& v = s->views[q];
-            acc += (long long)v.g.Nz * v.g.Ny * v.nxb;
-        }
-    }
-    s->task0[s->cap] = acc;
-    SCK(cudaMemcpyAsync(s->d_task0, s->task0.data(), sizeof(long long) * (s->cap + 1),
-                        cudaMemcpyDefault, s->stream));
-    SCK(cudaStreamSynchronize(s->stream));
-    return FDTD_OK;
-}
-
+// One branch per admitted request, forked from the engine stream and joined
+// back: L time steps of the request's own launches.
 int serve_capture_graph(FDTDServe* s) {
+    if (s->exec) { cudaGraphExecDestroy(s->exec); s->exec = nullptr; }
+    if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
+    std::vector<int> act;
+    for (int q = 0; q < s->cap; q++)
+        if (s->slot_h[q]) act.push_back(q);
+    s->dirty = false;
+    if (act.empty()) return FDTD_OK;
+    while (s->aux.size() < act.size()) {
+        cudaStream_t b = nullptr;
+        cudaEvent_t ev = nullptr;
+        SCK(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
+        s->aux.push_back(b);
+        SCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        s->join.push_back(ev);
+    }
     SCK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaSuccess;
-    for (int q = 0; q < s->L && e == cudaSuccess; q++)
-        e = fdtdb::launch_serve_step<float>(s->d_views, s->d_ctl, s->d_task0, s->cap, s->step_ctas,
-                                           s->copy_ctas, s->d_cap, s->stream);
+    cudaError_t e = cudaEventRecord(s->fork, s->stream);
+    for (size_t k = 0; k < act.size() && e == cudaSuccess; k++) {
+        cudaStream_t b = s->aux[k];
+        e = cudaStreamWaitEvent(b, s->fork, 0);
+        for (int q = 0; q < s->L && e == cudaSuccess; q++)
+            e = fdtdb::launch_serve_request_step<float>(s->views[act[k]], s->d_ctl + act[k], b);
+        if (e == cudaSuccess) e = cudaEventRecord(s->join[k], b);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s->stream, s->join[k], 0);
+    }
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
-    if (e != cudaSuccess) return s->cuda_fail(e, "serve step capture");
-    if (e2 != cudaSuccess) return s->cuda_fail(e2, "cudaStreamEndCapture");
+    if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        s->dirty = true;
+        return s->cuda_fail(e, "serve step capture");
+    }
+    if (e2 != cudaSuccess) {
+        s->dirty = true;
+        return s->cuda_fail(e2, "cudaStreamEndCapture");
+    }
     s->graph = g;
-    SCK(cudaGraphInstantiate(&s->exec, g, 0));
+    e = cudaGraphInstantiate(&s->exec, g, 0);
+    if (e != cudaSuccess) {
+        s->exec = nullptr;
+        s->dirty = true;
+        return s->cuda_fail(e, "cudaGraphInstantiate");
+    }
     return FDTD_OK;
 }
 
@@ -137,32 +157,22 @@ extern "C" FDTDServe* FDTD_serve_new(int device, double budget_bytes, int max_re
     s->cap = max_requests;
     s->L = steps_per_replay;
     cudaError_t e = cudaSetDevice(device);
-    int nsm = 0;
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_views, sizeof(fdtdb::ServeView<float>) * s->cap);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_ctl, sizeof(fdtdb::ServeCtl) * s->cap);
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_task0, sizeof(long long) * (s->cap + 1));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_cap, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_cap, 0, sizeof(int), s->stream);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_ctl, sizeof(fdtdb::ServeCtl) * s->cap);
     if (e != cudaSuccess) {
         s->cuda_fail(e, "FDTD_serve_new");
         return s;
     }
-    s->step_ctas = nsm * fdtdb::serve_step_ctas_per_sm<float>();   // one resident wave
-    s->copy_ctas = nsm * 4;
     s->views.assign(s->cap, fdtdb::ServeView<float>());
-    s->task0.assign(s->cap + 1, 0);
     s->slot_h.assign(s->cap, nullptr);
     s->slot_bytes.assign(s->cap, 0);
     s->admitted_step.assign(s->cap, 0);
     std::memset(s->h_ctl, 0, sizeof(fdtdb::ServeCtl) * s->cap);
     e = cudaMemcpyAsync(s->d_ctl, s->h_ctl, sizeof(fdtdb::ServeCtl) * s->cap, cudaMemcpyDefault, s->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_views, 0, sizeof(fdtdb::ServeView<float>) * s->cap, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) { s->cuda_fail(e, "FDTD_serve_new"); return s; }
-    if (serve_capture_graph(s) != FDTD_OK) return s;
-    if (serve_upload_tables(s) != FDTD_OK) return s;
     s->status = FDTD_OK;
     return s;
 }
@@ -272,13 +282,13 @@ extern "C" int FDTD_serve_admit(FDTDServe* s, FDTDHandle* h, const FDTDSolveOpti
     c.phi_change = 1;
     // first pass of the loop of emopt/fdtd.py:1016-1194 at n = 0
     c.state = (Tn - 1 > last) ? fdtdb::SERVE_TAIL : fdtdb::SERVE_RUN;
-    SCK(cudaMemcpyAsync(s->d_views + slot, &v, sizeof(v), cudaMemcpyDefault, s->stream));
     SCK(cudaMemcpyAsync(s->d_ctl + slot, &c, sizeof(c), cudaMemcpyDefault, s->stream));
+    SCK(cudaStreamSynchronize(s->stream));
     s->slot_h[slot] = h;
     s->slot_bytes[slot] = resident_bytes(r);
     s->used += s->slot_bytes[slot];
     s->admitted_step[slot] = s->replays;
-    if (serve_upload_tables(s) != FDTD_OK) return -s->status;
+    s->dirty = true;
     s->status = FDTD_OK;
     s->message.clear();
     return slot;
@@ -290,9 +300,10 @@ extern "C" int FDTD_serve_admit(FDTDServe* s, FDTDHandle* h, const FDTDSolveOpti
 extern "C" int FDTD_serve_advance(FDTDServe* s) {
     if (!s) return -FDTD_ERR_ARG;
     NvtxRange range("FDTD_serve_advance");
-    if (!s->exec) return -s->fail(FDTD_ERR_CUDA, "engine not initialised");
+    if (!s->d_ctl) return -s->fail(FDTD_ERR_CUDA, "engine not initialised");
     SCK(cudaSetDevice(s->device));
-    SCK(cudaGraphLaunch(s->exec, s->stream));
+    if (s->dirty && serve_capture_graph(s) != FDTD_OK) return -s->status;
+    if (s->exec) SCK(cudaGraphLaunch(s->exec, s->stream));
     SCK(cudaMemcpyAsync(s->h_ctl, s->d_ctl, sizeof(fdtdb::ServeCtl) * s->cap, cudaMemcpyDefault, s->stream));
     SCK(cudaStreamSynchronize(s->stream));
     s->replays++;
@@ -353,7 +364,7 @@ extern "C" int FDTD_serve_collect(FDTDServe* s, FDTDHandle** done, FDTDSolveResu
         o.A_change = c.A_change;
         o.phi_change = c.phi_change;
         o.nprobes = c.nprobes;
-        o.launches = (s->replays - s->admitted_step[q]) * (long long)s->L * 4;
+        o.launches = (s->replays - s->admitted_step[q]) * (long long)s->L * 3;
         o.status = FDTD_OK;
         if (!c.fixed) {
             const bool bad = std::isnan(c.A_change) || std::isinf(c.A_change) ||
@@ -374,7 +385,7 @@ extern "C" int FDTD_serve_collect(FDTDServe* s, FDTDHandle** done, FDTDSolveResu
         s->slot_h[q] = nullptr;
         changed = true;
     }
-    if (changed && serve_upload_tables(s) != FDTD_OK) return -s->status;
+    if (changed) s->dirty = true;
     return k;
 }
 
@@ -395,10 +406,10 @@ extern "C" void FDTD_serve_delete(FDTDServe* s) {
         if (s->slot_h[q]) s->slot_h[q]->r32.release_all();
     if (s->exec) cudaGraphExecDestroy(s->exec);
     if (s->graph) cudaGraphDestroy(s->graph);
-    if (s->d_views) cudaFree(s->d_views);
+    for (auto b : s->aux) cudaStreamDestroy(b);
+    for (auto ev : s->join) cudaEventDestroy(ev);
+    if (s->fork) cudaEventDestroy(s->fork);
     if (s->d_ctl) cudaFree(s->d_ctl);
-    if (s->d_task0) cudaFree(s->d_task0);
-    if (s->d_cap) cudaFree(s->d_cap);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;

@@ -21,8 +21,11 @@
 //     step(n, 1, part 2); [start the E exchange]
 //
 // The field arrays carry one halo plane below and above the slab; the
-// exchange writes into them (FDTD_slab_halo gives the device addresses).  The
-// vector kernels read a halo plane where the slab has a neighbour and apply
+// exchange writes into them (FDTD_slab_halo gives the device addresses).
+// Slabs that share a device and a stream need no exchange: each can read its
+// neighbours' boundary planes in place (FDTD_slab_set_halo_source), stream
+// order putting every H half step of a step before every E half step.  The
+// vector kernels read a neighbour plane where the slab has a neighbour and apply
 // the boundary rule of the global grid where it has none, and take the z CPML
 // coefficient of the global plane, so every cell is updated exactly as in the
 // single-GPU solve.  The convergence probe works on the probe values of all
@@ -46,6 +49,13 @@ fdtdb::GridView<T> slab_view(FDTDHandle* h, Resident<T>& r) {
     g.pml[2].edge_max = h->slab_Nz - h->w[5];
     g.zlo = (char)(h->slab_lo ? 1 : 0);
     g.zhi = (char)(h->slab_hi ? 1 : 0);
+    // the neighbour planes: the slab's own halo planes unless
+    // FDTD_slab_set_halo_source named other ones
+    const long long plane = (long long)r.Ny * r.px;
+    const T* own[4] = {dptr<T>(r.F[0][0]) + (h->Nz + 1) * plane, dptr<T>(r.F[0][1]) + (h->Nz + 1) * plane,
+                       dptr<T>(r.F[0][3]), dptr<T>(r.F[0][4])};
+    for (int c = 0; c < 4; c++)
+        g.zhalo[c] = h->slab_zhalo[c] ? static_cast<const T*>(h->slab_zhalo[c]) : own[c];
     return g;
 }
 
@@ -257,6 +267,7 @@ extern "C" int FDTD_slab_set(FDTDHandle* h, int i0, int Nz_global, int has_lo, i
     h->slab_Nz = Nz_global;
     h->slab_lo = has_lo ? 1 : 0;
     h->slab_hi = has_hi ? 1 : 0;
+    for (int c = 0; c < 4; c++) h->slab_zhalo[c] = nullptr;   // the slab's own halo planes
     return FDTD_OK;
 }
 
@@ -291,6 +302,17 @@ extern "C" int FDTD_slab_step_part(FDTDHandle* h, long long n, int half, int par
                  : FDTD_ERR_ARG;
     return h->precision == 32 ? slab_step_impl<float>(h, n, half, part)
                               : slab_step_impl<double>(h, n, half, part);
+}
+
+extern "C" int FDTD_slab_set_halo_source(FDTDHandle* h, void* const* ptrs) {
+    if (!h || !ptrs) return h ? h->fail(FDTD_ERR_ARG, "FDTD_slab_set_halo_source: null argument") : FDTD_ERR_ARG;
+    if (!h->slab) return h->fail(FDTD_ERR_ARG, "FDTD_slab_set_halo_source: not a slab (FDTD_slab_set)");
+    if ((ptrs[0] || ptrs[1]) && !h->slab_hi)
+        return h->fail(FDTD_ERR_ARG, "FDTD_slab_set_halo_source: no slab above to read from");
+    if ((ptrs[2] || ptrs[3]) && !h->slab_lo)
+        return h->fail(FDTD_ERR_ARG, "FDTD_slab_set_halo_source: no slab below to read from");
+    for (int c = 0; c < 4; c++) h->slab_zhalo[c] = ptrs[c];
+    return FDTD_OK;
 }
 
 extern "C" int FDTD_slab_halo(FDTDHandle* h, void** ptrs, long long* plane_elems) {

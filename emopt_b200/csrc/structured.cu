@@ -287,8 +287,13 @@ extern "C" int FDTD_structured_values(int device, void* stream, const double* zs
         if (!(zs[l] <= zs[l + 1])) return fail(FDTD_ERR_ARG, "layer boundaries must ascend");
     for (int q = 0; q < nprims; q++) {
         const int* pi = prim_info + 4 * q;
-        if (pi[0] < 0 || pi[1] < 3 || pi[0] + pi[1] > nverts || pi[2] < 0 || pi[3] < 1 || pi[2] + pi[3] > nparts)
+        // a circle: outline count -1, centre and radius in two vertex slots, no parts
+        const bool circle = pi[1] == -1;
+        const int nv = circle ? 2 : pi[1];
+        if (pi[0] < 0 || (!circle && nv < 3) || pi[0] + nv > nverts || pi[2] < 0 ||
+            (circle ? pi[3] != 0 : pi[3] < 1) || pi[2] + pi[3] > nparts)
             return fail(FDTD_ERR_ARG, "bad primitive table");
+        if (circle && !(verts[2 * pi[0] + 2] >= 0.0)) return fail(FDTD_ERR_ARG, "bad circle radius");
     }
     for (int q = 0; q < nparts; q++)
         if (parts[2 * q] < 0 || parts[2 * q + 1] < 3 || parts[2 * q] + parts[2 * q + 1] > nverts)

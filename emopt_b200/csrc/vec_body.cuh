@@ -17,7 +17,8 @@
 // array first; a lane out of range records the site (GridView::chk) and
 // skips its accesses.  In a z slab
 // of a distributed solve (g.zlo / g.zhi) the neighbour plane across an inner
-// slab face is read from the halo plane of the field arrays, and the z CPML
+// slab face is read through g.zhalo (the slab's halo plane, or the
+// neighbouring slab's boundary plane on the same device), and the z CPML
 // index is taken at the global plane i + g.pml[2].off.
 #pragma once
 
@@ -97,6 +98,22 @@ __device__ __forceinline__ bool sources_touch(const SourceList<T>& src, int comp
     return hit;
 }
 
+// Does the warp that updates rows j0 .. j0+NR-1 of plane i, vectors 32 xb ..
+// 32 xb + 31, touch no CPML slab and no source box of the half step
+// (comp_base 3: H sources, 0: E sources)?  Then the body built without CPML
+// and source code (GEN = false) computes the same values in the same order.
+template <typename T, int NR>
+__device__ __forceinline__ bool plain_warp(const GridView<T>& g, const SourceList<T>& src,
+                                           int comp_base, int i, int j0, int xb) {
+    constexpr int V = V16<T>::N;
+    if (slab_local(g.pml[2], i + g.pml[2].off, true) >= 0) return false;
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+        if (j0 + r < g.Ny && slab_local(g.pml[1], j0 + r, false) >= 0) return false;
+    if (xb * 32 * V < g.pml[0].w0 || (xb + 1) * 32 * V - 1 >= g.pml[0].edge_max) return false;
+    return !(src.n && sources_touch<T>(src, comp_base, i, j0, j0 + NR, xb * 32 * V, (xb + 1) * 32 * V));
+}
+
 #ifdef FDTD_BOUNDS_CHECK
 // Debug builds: is idx in [lo, hi)?  The first failure records its site.
 template <typename T>
@@ -111,10 +128,10 @@ template <typename T>
 __device__ bool h_fields_ok(const GridView<T>& g, int i, int j, int k0, int lane, long long p) {
     constexpr int V = V16<T>::N;
     const long long plane = g.plane, top = (long long)g.Nz * plane;
-    const long long fhi = ((long long)g.Nz + (g.zhi ? 1 : 0)) * plane;
     bool ok = in_range(g, p, 0, top - V + 1, 1);
     if (j + 1 < g.Ny) ok &= in_range(g, p + g.px, 0, top - V + 1, 2);
-    if (i + 1 < g.Nz || g.zhi) ok &= in_range(g, p + plane, 0, fhi - V + 1, 3);
+    if (i + 1 < g.Nz) ok &= in_range(g, p + plane, 0, top - V + 1, 3);
+    else if (g.zhi) ok &= in_range(g, p - (long long)i * plane, 0, plane - V + 1, 3);
     if (lane == 31 && k0 + V < g.Nx) ok &= in_range(g, p + V, 0, top, 4);
     return ok;
 }
@@ -124,10 +141,10 @@ template <typename T>
 __device__ bool e_fields_ok(const GridView<T>& g, int i, int j, int k0, int lane, long long p) {
     constexpr int V = V16<T>::N;
     const long long plane = g.plane, top = (long long)g.Nz * plane;
-    const long long flo = g.zlo ? -plane : 0;
     bool ok = in_range(g, p, 0, top - V + 1, 11);
     if (j > 0) ok &= in_range(g, p - g.px, 0, top - V + 1, 12);
-    if (i > 0 || g.zlo) ok &= in_range(g, p - plane, flo, top - V + 1, 13);
+    if (i > 0) ok &= in_range(g, p - plane, 0, top - V + 1, 13);
+    else if (g.zlo) ok &= in_range(g, p, 0, plane - V + 1, 13);
     if (lane == 0 && k0 > 0) ok &= in_range(g, p - 1, 0, top, 14);
     return ok;
 }
@@ -140,10 +157,11 @@ __device__ bool e_fields_ok(const GridView<T>& g, int i, int j, int k0, int lane
 // arithmetic, so NR = 2 keeps twice the bytes of one warp in flight; the rows
 // share the loads they have in common (the H update of row j reads E of row
 // j+1, the E update of row j reads H of row j-1).
-template <typename T, int NR = 1>
+template <typename T, int NR = 1, bool GEN = true, bool SERVE = false>
 __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<T>& f,
                                      const SourceList<T>& src, const long long* step_ctr,
-                                     int off, int i, int j0, int xb, int lane) {
+                                     int off, int i, int j0, int xb, int lane,
+                                     const ServeGate<T>* sg = nullptr) {
     constexpr int V = vecb::V16<T>::N;
     constexpr unsigned FULL = 0xffffffffu;
     const int m = xb * 32 + lane;
@@ -152,7 +170,7 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
     const PmlAxis<T>& PX = g.pml[0];
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
-    const int lz0 = slab_local(PZ, i + PZ.off, true);   // same for every row of the warp
+    const int lz0 = GEN ? slab_local(PZ, i + PZ.off, true) : -1;   // same for every row of the warp
     bool act[NR];
     int p[NR], ly[NR], lz[NR];
 #pragma unroll
@@ -161,7 +179,7 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
         // lanes beyond the row still take part in the shuffles below
         const bool act0 = j < Ny && k0 < g.Nx;
         p[r] = act0 ? (i * Ny + j) * px + k0 : 0;
-        const int ly0 = slab_local(PY, j, false);
+        const int ly0 = GEN ? slab_local(PY, j, false) : -1;
 #ifdef FDTD_BOUNDS_CHECK
         // a lane whose indices fall outside their arrays records the site and skips
         act[r] = act0 && vecb::h_fields_ok(g, i, j, k0, lane, p[r]);
@@ -176,7 +194,7 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
 #endif
     }
     // does any lane of the warp touch an x slab?  (the same for all lanes)
-    const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
+    const bool xw = GEN && (xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max);
 
     if (g.pf > 0 && i + g.pf < Nz && xb * 32 * V < g.Nx) {
 #pragma unroll
@@ -187,6 +205,10 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
                 for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
             }
     }
+
+    // a served request's state and capture flag, read with the fields
+    int sstate = SERVE_RUN, scap = 0;
+    if (SERVE) { sstate = __ldg(sg->state); scap = __ldg(sg->capture); }
 
     // ---- every load of the thread first
     T ex[NR][V], ey[NR][V], ez[NR][V], exj[NR][V], ezj[NR][V], exi[NR][V], eyi[NR][V];
@@ -205,7 +227,8 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
             vecb::vload<T>(ex[r], f.c[0] + q); vecb::vload<T>(ey[r], f.c[1] + q); vecb::vload<T>(ez[r], f.c[2] + q);
             // E of row j+1: the next row's own load, or a load of its own for the last row
             if (r + 1 == NR && j + 1 < Ny) { vecb::vload<T>(exj[r], f.c[0] + q + px); vecb::vload<T>(ezj[r], f.c[2] + q + px); }
-            if (i + 1 < Nz || g.zhi) { vecb::vload<T>(exi[r], f.c[0] + q + Ny * px); vecb::vload<T>(eyi[r], f.c[1] + q + Ny * px); }
+            if (i + 1 < Nz) { vecb::vload<T>(exi[r], f.c[0] + q + Ny * px); vecb::vload<T>(eyi[r], f.c[1] + q + Ny * px); }
+            else if (g.zhi) { vecb::vload<T>(exi[r], g.zhalo[0] + (q - i * Ny * px)); vecb::vload<T>(eyi[r], g.zhalo[1] + (q - i * Ny * px)); }
             vecb::vload<T>(hx[r], f.c[3] + q); vecb::vload<T>(hy[r], f.c[4] + q); vecb::vload<T>(hz[r], f.c[5] + q);
             if (lane == 31 && k0 + V < g.Nx) { ey_n[r] = ld(f.c[1] + q + V); ez_n[r] = ld(f.c[2] + q + V); }
             if (ly[r] >= 0) {
@@ -255,7 +278,21 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
             for (int e = 0; e < V; e++) { mx[r][e] = g.bH[0]; my[r][e] = g.bH[1]; mz[r][e] = g.bH[2]; }
         }
     }
-    const bool srcb = src.n && vecb::sources_touch<T>(src, 3, i, j0, j0 + NR,
+    if (SERVE) {
+        // the whole warp leaves together (one state per request)
+        if (!serve_running(sstate)) return;
+        if (scap == 1 || scap == 2) {
+            T* const* d = sg->snap[scap - 1];
+#pragma unroll
+            for (int r = 0; r < NR; r++)
+                if (act[r]) {
+                    const int q = p[r];
+                    vecb::vstore<T>(d[0] + q, ex[r]); vecb::vstore<T>(d[1] + q, ey[r]); vecb::vstore<T>(d[2] + q, ez[r]);
+                    vecb::vstore<T>(d[3] + q, hx[r]); vecb::vstore<T>(d[4] + q, hy[r]); vecb::vstore<T>(d[5] + q, hz[r]);
+                }
+        }
+    }
+    const bool srcb = GEN && src.n && vecb::sources_touch<T>(src, 3, i, j0, j0 + NR,
                                                 xb * 32 * V, (xb + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_ctr + off];
@@ -331,10 +368,11 @@ __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<
     }
 }
 
-template <typename T, int NR = 1>
+template <typename T, int NR = 1, bool GEN = true, bool SERVE = false>
 __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<T>& f,
                                      const SourceList<T>& src, const long long* step_ctr,
-                                     int off, int i, int j0, int xb, int lane) {
+                                     int off, int i, int j0, int xb, int lane,
+                                     const ServeGate<T>* sg = nullptr) {
     constexpr int V = vecb::V16<T>::N;
     constexpr unsigned FULL = 0xffffffffu;
     const int m = xb * 32 + lane;
@@ -343,7 +381,7 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
     const PmlAxis<T>& PX = g.pml[0];
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
-    const int lz0 = slab_local(PZ, i + PZ.off, true);   // same for every row of the warp
+    const int lz0 = GEN ? slab_local(PZ, i + PZ.off, true) : -1;   // same for every row of the warp
     bool act[NR];
     int p[NR], ly[NR], lz[NR];
 #pragma unroll
@@ -351,7 +389,7 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
         const int j = j0 + r;
         const bool act0 = j < Ny && k0 < g.Nx;
         p[r] = act0 ? (i * Ny + j) * px + k0 : 0;
-        const int ly0 = slab_local(PY, j, false);
+        const int ly0 = GEN ? slab_local(PY, j, false) : -1;
 #ifdef FDTD_BOUNDS_CHECK
         act[r] = act0 && vecb::e_fields_ok(g, i, j, k0, lane, p[r]);
         ly[r] = (ly0 >= 0 && act[r] && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
@@ -365,7 +403,7 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
 #endif
     }
     // does any lane of the warp touch an x slab?  (the same for all lanes)
-    const bool xw = xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max;
+    const bool xw = GEN && (xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max);
     const bool lossy = g.aE[0] != nullptr;
 
     if (g.pf > 0 && i + g.pf < g.Nz && xb * 32 * V < g.Nx) {
@@ -379,6 +417,9 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
                 for (int c = 0; c < 3; c++) vecb::l2_prefetch<T>(g.bE[c] + q, lane, px - xb * 32 * V);
             }
     }
+
+    int sstate = SERVE_RUN;
+    if (SERVE) sstate = __ldg(sg->state);
 
     // ---- every load of the thread first
     T hx[NR][V], hy[NR][V], hz[NR][V], hxj[NR][V], hzj[NR][V], hxi[NR][V], hyi[NR][V];
@@ -398,7 +439,8 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
             vecb::vload<T>(bx[r], g.bE[0] + q); vecb::vload<T>(by[r], g.bE[1] + q); vecb::vload<T>(bz[r], g.bE[2] + q);
             // H of row j-1: the previous row's own load, or a load of its own for the first row
             if (r == 0 && j > 0) { vecb::vload<T>(hxj[r], f.c[3] + q - px); vecb::vload<T>(hzj[r], f.c[5] + q - px); }
-            if (i > 0 || g.zlo) { vecb::vload<T>(hxi[r], f.c[3] + q - Ny * px); vecb::vload<T>(hyi[r], f.c[4] + q - Ny * px); }
+            if (i > 0) { vecb::vload<T>(hxi[r], f.c[3] + q - Ny * px); vecb::vload<T>(hyi[r], f.c[4] + q - Ny * px); }
+            else if (g.zlo) { vecb::vload<T>(hxi[r], g.zhalo[2] + q); vecb::vload<T>(hyi[r], g.zhalo[3] + q); }
             if (lane == 0 && k0 > 0) { hy_p[r] = ld(f.c[4] + q - 1); hz_p[r] = ld(f.c[5] + q - 1); }
             if (ly[r] >= 0) {
                 const int s = (i * PY.wsum + ly[r]) * px + k0;
@@ -438,7 +480,8 @@ __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<
 #pragma unroll
             for (int e = 0; e < V; e++) { hxj[r][e] = hx[r - 1][e]; hzj[r][e] = hz[r - 1][e]; }
         }
-    const bool srcb = src.n && vecb::sources_touch<T>(src, 0, i, j0, j0 + NR,
+    if (SERVE && !serve_running(sstate)) return;   // the whole warp leaves together
+    const bool srcb = GEN && src.n && vecb::sources_touch<T>(src, 0, i, j0, j0 + NR,
                                                 xb * 32 * V, (xb + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_ctr + off];

@@ -39,12 +39,20 @@ __device__ __forceinline__ int vec_row() {
 #endif
 #define VEC_MINB(T) (sizeof(T) == 8 ? 18 : VEC_MINB32)
 
+// float32 warps whose cells lie in no CPML slab and no source box run a body
+// compiled without that code (vecb::plain_warp; 120.2 instead of 121.1 us per
+// step on the MMI block: the bodies wait on their loads more than they issue);
+// float64 keeps one body (a second one gained nothing: 199-200 us either way).
 template <typename T>
 __global__ void __launch_bounds__(sizeof(T) == 8 || VEC_MINB32 ? 32 * VEC_BLOCK_ROWS : 256, VEC_MINB(T))
 k_update_H_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
                int i0) {
-    vec_update_H<T, VEC_WARP_ROWS(T)>(g, f, src, step_base, off, i0 + (int)blockIdx.z, vec_row<T>(),
-                                      blockIdx.x, threadIdx.x);
+    constexpr int NR = VEC_WARP_ROWS(T);
+    const int i = i0 + (int)blockIdx.z, j0 = vec_row<T>();
+    if (sizeof(T) == 4 && vecb::plain_warp<T, NR>(g, src, 3, i, j0, blockIdx.x))
+        vec_update_H<T, NR, false>(g, f, src, step_base, off, i, j0, blockIdx.x, threadIdx.x);
+    else
+        vec_update_H<T, NR, true>(g, f, src, step_base, off, i, j0, blockIdx.x, threadIdx.x);
 }
 
 // The E kernel is bounded by its real block size: that keeps it at 64
@@ -53,8 +61,12 @@ template <typename T>
 __global__ void __launch_bounds__(32 * VEC_BLOCK_ROWS, VEC_MINB(T))
 k_update_E_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
                int i0) {
-    vec_update_E<T, VEC_WARP_ROWS(T)>(g, f, src, step_base, off, i0 + (int)blockIdx.z, vec_row<T>(),
-                                      blockIdx.x, threadIdx.x);
+    constexpr int NR = VEC_WARP_ROWS(T);
+    const int i = i0 + (int)blockIdx.z, j0 = vec_row<T>();
+    if (sizeof(T) == 4 && vecb::plain_warp<T, NR>(g, src, 0, i, j0, blockIdx.x))
+        vec_update_E<T, NR, false>(g, f, src, step_base, off, i, j0, blockIdx.x, threadIdx.x);
+    else
+        vec_update_E<T, NR, true>(g, f, src, step_base, off, i, j0, blockIdx.x, threadIdx.x);
 }
 
 template <typename T>

@@ -194,7 +194,9 @@ def dfdx_interp(domain, dF: dict, bc: str):
 
 
 # ------------------------------------------------------------- source power
-_FLUX = {0: ("Ey", "Hz", "Ez", "Hy"), 1: ("Ex", "Hz", "Ez", "Hx"), 2: ("Ex", "Hy", "Ey", "Hx")}
+# (E1, H2, E2, H1) with Re(E1 H2* - E2 H1*) = Re(E x H*) . n through a plane
+# normal to x, y, z (the kernel's kFluxComps)
+_FLUX = {0: ("Ey", "Hz", "Ez", "Hy"), 1: ("Ez", "Hx", "Ex", "Hz"), 2: ("Ex", "Hy", "Ey", "Hx")}
 
 
 def _flux_sums(raws, geoms, axes) -> torch.Tensor:

@@ -118,6 +118,7 @@ class CudaSlab:
         self.Nx, self.Ny, self.Nz, self.i0, self.I = Nx, Ny, Nz, i0, I
         self.dt = prm["dt"]
         self.device = device
+        self.stream = stream
         self.dtype = np.float32 if precision == "fp32" else np.float64
         h = libFDTD.FDTD_new()
         self.h = h
@@ -195,6 +196,15 @@ class CudaSlab:
         self._ok(libFDTD.FDTD_slab_sample(self.h, ctypes.byref(sp)), "FDTD_slab_sample")
         self.samples = _device_tensor(sp.value, 3 * max(len(cells), 1), np.float64, self.device)
 
+    def set_halo_source(self, above=None, below=None):
+        """Read the neighbour planes from other planes of this device:
+        ``above`` = (Ex, Ey) of the plane above the slab, ``below`` = (Hx, Hy)
+        of the plane below (tensors); None keeps the slab's own halo planes
+        (FDTD_slab_set_halo_source)."""
+        ptrs = (ctypes.c_void_p * 4)(*([t.data_ptr() for t in above] if above else [None, None]),
+                                     *([t.data_ptr() for t in below] if below else [None, None]))
+        self._ok(libFDTD.FDTD_slab_set_halo_source(self.h, ptrs), "FDTD_slab_set_halo_source")
+
     def half_step(self, n: int, half: int):
         self._ok(libFDTD.FDTD_slab_step(self.h, n, half), "FDTD_slab_step")
 
@@ -230,36 +240,100 @@ class CudaSlab:
 
 
 class LocalLink:
-    """Slabs of one process: halo planes and probe sums move by device copies."""
+    """Slabs of one process: halo planes and probe sums move by device copies.
 
-    # the copies run in stream order on the device: splitting the half steps
-    # to overlap them would only add launches
-    overlap = False
+    Direct (``direct=True``, every slab on one device and one stream): no
+    copies at all -- each slab's half steps read the neighbour planes in the
+    neighbouring slabs' own arrays (``attach``, FDTD_slab_set_halo_source);
+    stream order puts every H half step of a step before every E half step.
+    Plain (``overlap=False``): the copies run in stream order on the slabs'
+    stream, between the half steps.  Overlapped: each copy runs on a side
+    stream of the receiving device, after everything queued so far on the
+    sending slab's stream, and the receiving slab's stream waits for it only
+    before the plane that reads the halo; the half steps run in two parts
+    around it like the NCCL transport's."""
 
-    def __init__(self, slabs):
+    def __init__(self, slabs, overlap=False, direct=False):
+        if direct and overlap:
+            raise ValueError("direct halo reads need no exchange to overlap")
+        if direct and len({(s.device, s.stream) for s in slabs}) > 1:
+            raise ValueError("direct halo reads need all slabs on one device and one stream")
         self.slabs = slabs
+        self.direct = bool(direct)
+        self.overlap = bool(overlap)
+        self._sides = {}
+        self._streams = {}
+        self._pending = {"E": [], "H": []}
+        if self.overlap and any(s.stream is None for s in slabs):
+            raise ValueError("overlapped device copies need the slabs' streams")
+
+    def _stream(self, slab):
+        st = self._streams.get(id(slab))
+        if st is None:
+            import torch
+            st = self._streams[id(slab)] = torch.cuda.ExternalStream(
+                slab.stream, device=torch.device("cuda", slab.device))
+        return st
+
+    def attach(self):
+        """Direct mode: point every slab at its neighbours' boundary planes
+        (after every slab's begin, which places its arrays)."""
+        if not self.direct:
+            return
+        for q, s in enumerate(self.slabs):
+            above = self.slabs[q + 1].halo["E_send"] if q + 1 < len(self.slabs) else None
+            below = self.slabs[q - 1].halo["H_send"] if q > 0 else None
+            s.set_halo_source(above, below)
+
+    def _start(self, which, pairs):
+        """pairs: (receiving slab, destination, sending slab, source)."""
+        if self.direct:
+            return
+        if not self.overlap:
+            for _, dst, _, src in pairs:
+                dst.copy_(src)
+            return
+        import torch
+        done = []
+        for rs, dst, ss, src in pairs:
+            side = self._sides.get(rs.device)
+            if side is None:
+                side = self._sides[rs.device] = torch.cuda.Stream(device=torch.device("cuda", rs.device))
+            # the source plane is written, and the previous reader of the
+            # destination has run, by everything queued so far
+            side.wait_stream(self._stream(ss))
+            side.wait_stream(self._stream(rs))
+            with torch.cuda.stream(side):
+                dst.copy_(src, non_blocking=True)
+            done.append((rs, side.record_event()))
+        self._pending[which] = done
+
+    def _wait(self, which):
+        for rs, ev in self._pending[which]:
+            self._stream(rs).wait_event(ev)
+        self._pending[which] = []
 
     def start_E(self):
-        for lo, hi in zip(self.slabs[:-1], self.slabs[1:]):
-            for c in range(2):
-                lo.halo["E_recv"][c].copy_(hi.halo["E_send"][c])
+        self._start("E", [(lo, lo.halo["E_recv"][c], hi, hi.halo["E_send"][c])
+                          for lo, hi in zip(self.slabs[:-1], self.slabs[1:]) for c in range(2)])
 
     def start_H(self):
-        for lo, hi in zip(self.slabs[:-1], self.slabs[1:]):
-            for c in range(2):
-                hi.halo["H_recv"][c].copy_(lo.halo["H_send"][c])
+        self._start("H", [(hi, hi.halo["H_recv"][c], lo, lo.halo["H_send"][c])
+                          for lo, hi in zip(self.slabs[:-1], self.slabs[1:]) for c in range(2)])
 
     def wait_E(self):
-        """The copies run in stream order: nothing to wait for."""
+        self._wait("E")
 
     def wait_H(self):
-        """The copies run in stream order: nothing to wait for."""
+        self._wait("H")
 
     def exchange_E(self):
         self.start_E()
+        self.wait_E()
 
     def exchange_H(self):
         self.start_H()
+        self.wait_H()
 
     def sum_samples(self, tensors):
         total = tensors[0].clone()
@@ -436,7 +510,7 @@ class SlabSet:
     """
 
     def __init__(self, p, ranges, precision="fp32", devices=None, link=None, rank=None,
-                 stream=None, t0_device=False):
+                 stream=None, t0_device=False, overlap=False, direct=None):
         prm = derive_parameters(p.X, p.Y, p.Z, p.dx, p.dy, p.dz, p.wavelength, 1.0, p.nconv or 10)
         Nx, Ny, Nz = prm["Nx"], prm["Ny"], prm["Nz"]
         self.p = p
@@ -465,13 +539,23 @@ class SlabSet:
             raise
         self.link = link
         self.rank = rank
+        self.overlap = overlap
+        # slabs of one process on one device read each other's planes
+        # directly unless told otherwise (or asked to overlap copies)
+        if direct is None:
+            direct = (rank is None and not overlap and len(self.slabs) > 1 and
+                      len({(s.device, s.stream) for s in self.slabs}) == 1)
+        self.direct = bool(direct)
         self.res = None
 
     def begin(self):
         for s in self.slabs:
             s.begin(self.Tn, self.p.fixed_steps, self.Nmax, self.cells)
         if self.link is None:
-            self.link = LocalLink(self.slabs) if self.rank is None else TorchLink(self.slabs[0])
+            self.link = (LocalLink(self.slabs, overlap=self.overlap, direct=self.direct)
+                         if self.rank is None else TorchLink(self.slabs[0]))
+        if hasattr(self.link, "attach"):
+            self.link.attach()
 
     def run(self, history=None) -> SlabResult:
         self.res = run(self.slabs, self.link, self.Tn, self.p.rtol, self.Nmax, self.p.fixed_steps,
@@ -525,10 +609,11 @@ def grad_eps_planar(fwd, adj, box, ranges, link, device=0):
     return total
 
 
-def solve(p, ranges, precision="fp32", devices=None, link=None, rank=None, stream=None):
+def solve(p, ranges, precision="fp32", devices=None, link=None, rank=None, stream=None,
+          overlap=False, direct=None):
     """Solve problem ``p`` split into the slabs ``ranges`` (see ``SlabSet``).
     Returns (result, {slab index: six complex [I, Ny, Nx] arrays})."""
-    ss = SlabSet(p, ranges, precision, devices, link, rank, stream)
+    ss = SlabSet(p, ranges, precision, devices, link, rank, stream, overlap=overlap, direct=direct)
     try:
         ss.begin()
         res = ss.run()

@@ -283,6 +283,14 @@ int FDTD_slab_step_part(FDTDHandle *h, long long n, int half, int part);
  * top plane (send up); ptrs[6..7] the Hx, Hy halo below (receive from below). */
 int FDTD_slab_halo(FDTDHandle *h, void **ptrs, long long *plane_elems);
 
+/* Where the half steps read the neighbour planes: ptrs[0..1] Ex, Ey of the
+ * plane above the slab, ptrs[2..3] Hx, Hy of the plane below (device
+ * addresses of Ny x px planes in the slab's precision, e.g. the neighbouring
+ * slab's ptrs[0..1] / ptrs[4..5] of FDTD_slab_halo when it lives on the same
+ * device: no exchange is then needed); NULL keeps the slab's own halo plane.
+ * Holds until the next call. */
+int FDTD_slab_set_halo_source(FDTDHandle *h, void *const *ptrs);
+
 /* Writes the probe values this slab holds (3 x npoints doubles, zero for the
  * points of other slabs) into a device buffer and returns its address; the
  * caller sums the buffers of all slabs into every slab's buffer. */
@@ -358,9 +366,9 @@ int FDTD_dfdx_interp(int device, void *stream, int comp, const fdtd_complex128 *
 
 /* Poynting sums of the source power (get_source_power, emopt/fdtd.py:1555-
  * 1667): for each of nplanes <= 6 planes, sum over its cells of
- * Re(E1 conj(H2) - E2 conj(H1)) -- (Ey, Hz, Ez, Hy) for axes[p] = 0, (Ex, Hz,
- * Ez, Hx) for 1, (Ex, Hy, Ey, Hx) for 2 -- every component interpolated as
- * FDTD_interp_field does.  blocks[6p + c]: component c of plane p's raw
+ * Re(E1 conj(H2) - E2 conj(H1)) = Re(E x H*) . n -- (Ey, Hz, Ez, Hy) for
+ * axes[p] = 0, (Ez, Hx, Ex, Hz) for 1, (Ex, Hy, Ey, Hx) for 2 -- every
+ * component interpolated as FDTD_interp_field does.  blocks[6p + c]: component c of plane p's raw
  * block; geoms: 17 ints per plane.  sums: device memory of at least
  * 6 + 6 * 148 doubles (partial sums); sums[p] receives plane p's sum, in a
  * fixed summation order. */

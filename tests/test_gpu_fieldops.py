@@ -10,7 +10,8 @@ the host forms with the reference's semantics:
 * interpolated_dFdx_3D on CUDA tensors == the numpy form
   (emopt/fomutils.py:1282-1426, quirks at symmetric min faces included);
 * source power == FDTD.get_source_power to 1e-12, and its gradient == autograd
-  through the torch restatement of the same sums.
+  through the torch restatement of the same sums, on a grid where all six
+  planes hold cells.
 The phasors are seeded random complex arrays written into the solver's t0
 arrays: the kernels are pure functions of them."""
 import itertools
@@ -31,10 +32,13 @@ pytestmark = pytest.mark.gpu
 COMPS = FO.COMPONENTS
 BCS = ["".join(t) + "0" for t in itertools.product("0EH", repeat=2)]
 SHAPE = (9, 11, 14)
+# every source-power plane holds cells on this grid (on SHAPE with these
+# CPML widths the planes normal to x and y are empty)
+POWER_SHAPE, POWER_PML = (14, 13, 16), (3, 4, 3, 2, 2, 3)
 
 
-def _sim(bc, seed=0):
-    p = P.random_box(seed, shape=SHAPE, w_pml=(3, 4, 3, 2, 3, 4), bc=bc)
+def _sim(bc, seed=0, shape=SHAPE, w_pml=(3, 4, 3, 2, 3, 4)):
+    p = P.random_box(seed, shape=shape, w_pml=w_pml, bc=bc)
     sim = P.make_solver(p, precision="fp64")
     rng = np.random.default_rng(seed + 17)
     for c in COMPS:
@@ -131,7 +135,10 @@ def test_dfdx_interp_matches_host_form(bc):
 def _power_inputs(sim, F):
     d = (sim.dx, sim.dy, sim.dz)
     planes = A.source_power_planes(sim)
-    grown = [FO.grow_domain(dom, SHAPE, d) for dom, _, _ in planes]
+    for dom, _, _ in planes:
+        assert dom.i2 > dom.i1 and dom.j2 > dom.j1 and dom.k2 > dom.k1
+    assert {axis for _, axis, _ in planes} == {0, 1, 2}
+    grown = [FO.grow_domain(dom, POWER_SHAPE, d) for dom, _, _ in planes]
     raws = [torch.stack([F[c][g.i1:g.i2, g.j1:g.j2, g.k1:g.k2] for c in COMPS]).contiguous()
             for g in grown]
     return planes, grown, raws
@@ -139,7 +146,7 @@ def _power_inputs(sim, F):
 
 @pytest.mark.parametrize("bc", BCS)
 def test_source_power_matches_host_form(bc):
-    sim = _sim(bc, seed=21 + BCS.index(bc))
+    sim = _sim(bc, seed=21 + BCS.index(bc), shape=POWER_SHAPE, w_pml=POWER_PML)
     planes, grown, raws = _power_inputs(sim, _fields(sim))
     ref = sim.get_source_power()
     got = float(FO.source_power(raws, planes, grown, sim))
@@ -148,7 +155,7 @@ def test_source_power_matches_host_form(bc):
 
 @pytest.mark.parametrize("bc", ["000", "EH0", "0E0"])
 def test_source_power_gradient_matches_autograd(bc):
-    sim = _sim(bc, seed=31)
+    sim = _sim(bc, seed=31, shape=POWER_SHAPE, w_pml=POWER_PML)
     planes, grown, raws = _power_inputs(sim, _fields(sim))
     r1 = [r.clone().requires_grad_(True) for r in raws]
     r2 = [r.clone().requires_grad_(True) for r in raws]

@@ -38,38 +38,33 @@ def _single(p, precision):
     return np.stack([sim._raw(c, False) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")]), info
 
 
-class OverlapLocalLink(zslab.LocalLink):
-    """Device copies with the overlapped schedule of the NCCL transport: every
-    half step in two parts (the planes that read no halo, then the plane next
-    to it, FDTD_slab_step_part) around the exchange."""
-    overlap = True
-
-
-def _slabs(p, nslab, precision, overlap=False):
+def _slabs(p, nslab, precision, mode="direct"):
+    """mode: "direct" (the slabs read each other's boundary planes in place),
+    "copy" (halo planes exchanged by device copies between the half steps) or
+    "overlap" (copies on a side stream, the half steps in two parts around
+    them)."""
     ranges = zslab.ownership(p.shape[0], nslab)
-    link = None
-    if overlap:
-        ss = zslab.SlabSet(p, ranges, precision=precision)
-        try:
-            ss.begin()
-            ss.link = OverlapLocalLink(ss.slabs)
-            res = ss.run()
-            parts = ss.finish()
-        finally:
-            ss.close()
-    else:
-        res, parts = zslab.solve(p, ranges, precision=precision, link=link)
+    ss = zslab.SlabSet(p, ranges, precision=precision, overlap=mode == "overlap",
+                       direct=None if mode == "direct" else False)
+    try:
+        ss.begin()
+        assert ss.link.direct == (mode == "direct") and ss.link.overlap == (mode == "overlap")
+        res = ss.run()
+        parts = ss.finish()
+    finally:
+        ss.close()
     F = np.stack([np.concatenate([parts[s][c] for s in range(len(ranges))]) for c in range(6)])
     return F, res
 
 
+@pytest.mark.parametrize("mode", ["direct", "copy"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_fixed_steps_equal_single_gpu_solve(name, precision):
+def test_fixed_steps_equal_single_gpu_solve(name, precision, mode):
     kw, nslab = CASES[name]
     p = P.random_box(**dict(kw, fixed_steps=150))
     F1, info = _single(p, precision)
-    F, res = _slabs(p, nslab, precision)
+    F, res = _slabs(p, nslab, precision, mode)
     assert res.steps == info["steps"] and res.n_main == info["n_main"]
     assert np.array_equal(F, F1)
 
@@ -82,7 +77,7 @@ def test_overlapped_schedule_equals_single_gpu_solve(name, precision):
     kw, nslab = CASES[name]
     p = P.random_box(**dict(kw, fixed_steps=150))
     F1, info = _single(p, precision)
-    F, res = _slabs(p, nslab, precision, overlap=True)
+    F, res = _slabs(p, nslab, precision, "overlap")
     assert res.steps == info["steps"] and res.n_main == info["n_main"]
     assert np.array_equal(F, F1)
 

@@ -150,3 +150,37 @@ def test_self_crossing_polygon_is_rejected():
     bowtie = G.Polygon([0, 1, 1, 0], [0, 1, 0, 1])
     with pytest.raises(ValueError, match="cross"):
         G._convex_parts(bowtie.outline())
+
+
+def _check_tables(mat, info=None):
+    """FDTD_structured_values on an empty cell range: the table checks run,
+    no device is touched."""
+    import ctypes
+    from emopt_b200.fdtd_ctypes import libFDTD
+    zs, start, flat, info0, vals, parts, verts, nprims, nparts, nverts = mat.tables()
+    info = info0 if info is None else info
+    msg = ctypes.create_string_buffer(256)
+    rc = libFDTD.FDTD_structured_values(
+        0, None, zs.ctypes.data, len(zs), start.ctypes.data, flat.ctypes.data, info.ctypes.data,
+        vals.ctypes.data, nprims, parts.ctypes.data, nparts, verts.ctypes.data, nverts,
+        1.0, 1.0, 1.0, 0, 0, 0, 4, 0, 4, 0.0, 0.0, 0.0, vals.ctypes.data, msg, 256)
+    return rc, msg.value.decode()
+
+
+@pytest.mark.parametrize("seed", [1, 3, 20, 21])
+def test_library_accepts_circle_tables(seed):
+    """Every table the host builds (circles included: outline count -1, no
+    convex parts) passes the library's table checks."""
+    mat, _ = _random_layout(seed, n=12, polygons=seed % 2 == 1, circles=True)
+    info = mat.tables()[3].reshape(-1, 4)
+    assert (info[:, 1] == -1).any()
+    assert _check_tables(mat) == (0, "")
+
+
+def test_library_rejects_bad_circle_entry():
+    mat, _ = _random_layout(20, n=12, polygons=False, circles=True)
+    info = mat.tables()[3].copy().reshape(-1, 4)
+    q = int(np.nonzero(info[:, 1] == -1)[0][0])
+    info[q, 3] = 1          # a circle carries no convex parts
+    rc, msg = _check_tables(mat, np.ascontiguousarray(info.reshape(-1)))
+    assert rc != 0 and "bad primitive table" in msg

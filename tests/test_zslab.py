@@ -151,3 +151,31 @@ def test_two_gloo_ranks_match_reference_multirank():
         assert A == ref["A_change"]
     for c in range(6):
         assert np.array_equal(np.concatenate([r[4][c] for r in res]), ref["fields"][c]), c
+
+
+def test_halo_source_checks_on_the_host():
+    """FDTD_slab_set_halo_source accepts neighbour planes only on the faces that
+    have a neighbour, and only on a slab handle (host-side checks; no device
+    work)."""
+    import ctypes
+    from emopt_b200 import fdtd_ctypes as ct
+    lib = ct.libFDTD
+    h = lib.FDTD_new()
+    try:
+        lib.FDTD_set_grid_dims(h, 10, 8, 4)
+        lib.FDTD_set_local_grid(h, 0, 0, 0, 10, 8, 4)
+        buf = ctypes.create_string_buffer(64)
+        some = ctypes.cast(buf, ctypes.c_void_p).value
+        none4 = (ctypes.c_void_p * 4)()
+        above = (ctypes.c_void_p * 4)(some, some, None, None)
+        below = (ctypes.c_void_p * 4)(None, None, some, some)
+        assert lib.FDTD_slab_set_halo_source(h, none4) == ct.FDTD_ERR_ARG        # not a slab
+        assert lib.FDTD_slab_set(h, 0, 12, 0, 1) == ct.FDTD_OK                    # bottom slab
+        assert lib.FDTD_slab_set_halo_source(h, below) == ct.FDTD_ERR_ARG         # nothing below
+        assert lib.FDTD_slab_set_halo_source(h, above) == ct.FDTD_OK
+        assert lib.FDTD_slab_set_halo_source(h, none4) == ct.FDTD_OK              # back to its own halo
+        assert lib.FDTD_slab_set(h, 8, 12, 1, 0) == ct.FDTD_OK                    # top slab
+        assert lib.FDTD_slab_set_halo_source(h, above) == ct.FDTD_ERR_ARG         # nothing above
+        assert lib.FDTD_slab_set_halo_source(h, below) == ct.FDTD_OK
+    finally:
+        lib.FDTD_delete(h)
