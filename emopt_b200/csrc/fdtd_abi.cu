@@ -1112,6 +1112,7 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
                                                 odd ? f0 : f1, src, sb, (int)q, zc, h->stream));
             } else if (vec) {
                 CK(fdtdb::launch_step_vec<T>(g0, f0, src, sb, (int)q, h->stream));
+
             } else {
                 fdtdb::launch_step_unfused<T>(g0, f0, src, sb, (int)q, h->stream);
             }

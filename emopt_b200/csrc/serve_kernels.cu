@@ -38,11 +38,11 @@ k_serve_half(GridView<T> g, Fields<T> f, SourceList<T> src, const __grid_constan
              const long long* step_ctr) {
     const int i = (int)blockIdx.z, j = (int)blockIdx.y, xb = (int)blockIdx.x;
     if (sizeof(T) == 4 && vecb::plain_warp<T, 1>(g, src, IS_E ? 0 : 3, i, j, xb)) {
-        if (IS_E) vec_update_E<T, 1, false, true>(g, f, src, step_ctr, 0, i, j, xb, threadIdx.x, &sg);
-        else vec_update_H<T, 1, false, true>(g, f, src, step_ctr, 0, i, j, xb, threadIdx.x, &sg);
+        if (IS_E) vec_update_E<T, false, true>(g, f, src, step_ctr, 0, i, j, xb, threadIdx.x, &sg);
+        else vec_update_H<T, false, true>(g, f, src, step_ctr, 0, i, j, xb, threadIdx.x, &sg);
     } else {
-        if (IS_E) vec_update_E<T, 1, true, true>(g, f, src, step_ctr, 0, i, j, xb, threadIdx.x, &sg);
-        else vec_update_H<T, 1, true, true>(g, f, src, step_ctr, 0, i, j, xb, threadIdx.x, &sg);
+        if (IS_E) vec_update_E<T, true, true>(g, f, src, step_ctr, 0, i, j, xb, threadIdx.x, &sg);
+        else vec_update_H<T, true, true>(g, f, src, step_ctr, 0, i, j, xb, threadIdx.x, &sg);
     }
 }
 

@@ -152,431 +152,437 @@ __device__ bool e_fields_ok(const GridView<T>& g, int i, int j, int k0, int lane
 
 }  // namespace vecb
 
-// Rows per warp: a warp updates the same 32 vectors of NR consecutive rows
-// j0 .. j0+NR-1 of plane i.  Every load of all rows is issued before any
-// arithmetic, so NR = 2 keeps twice the bytes of one warp in flight; the rows
-// share the loads they have in common (the H update of row j reads E of row
-// j+1, the E update of row j reads H of row j-1).
-template <typename T, int NR = 1, bool GEN = true, bool SERVE = false>
-__device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<T>& f,
-                                     const SourceList<T>& src, const long long* step_ctr,
-                                     int off, int i, int j0, int xb, int lane,
-                                     const ServeGate<T>* sg = nullptr) {
+// One warp task: the 32 vectors 32 xb .. 32 xb + 31 of row j of plane i.
+// Each body is a load phase (every index, then every load the task needs,
+// issued before any arithmetic) and a finish phase (the update and the
+// stores) around a register set of the task (HTask / ETask).  A task writes
+// only its own cells, and no array a half step writes is read by another
+// task of that half step, so tasks may run in any order.
+// GEN = false: the caller guarantees that the task touches no CPML slab and
+// no source box (vecb::plain_warp); the CPML and source code is compiled out.
+// SERVE: a served request's state gates the stores, and the H half step
+// writes the fields it read into a snapshot set on a capture step
+// (ServeGate).
+
+template <typename T>
+struct HTask {
+    static constexpr int V = vecb::V16<T>::N;
+    T ex[V], ey[V], ez[V], exj[V], ezj[V], exi[V], eyi[V], hx[V], hy[V], hz[V];
+    T py0[V], py1[V], pz0[V], pz1[V], px0[V], px1[V];
+    T mx[V], my[V], mz[V];
+    T ey_n, ez_n;
+    int lxs[V];
+    int p, ly, lz;
+    bool act;
+    int sstate, scap;
+};
+
+template <typename T, bool GEN = true, bool SERVE = false>
+__device__ __forceinline__ void h_load(const GridView<T>& g, const Fields<T>& f, int i, int j, int xb,
+                                       int lane, const ServeGate<T>* sg, HTask<T>& t) {
     constexpr int V = vecb::V16<T>::N;
-    constexpr unsigned FULL = 0xffffffffu;
     const int m = xb * 32 + lane;
     const int k0 = m * V;
     const int Ny = g.Ny, Nz = g.Nz, px = g.px;
     const PmlAxis<T>& PX = g.pml[0];
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
-    const int lz0 = GEN ? slab_local(PZ, i + PZ.off, true) : -1;   // same for every row of the warp
-    bool act[NR];
-    int p[NR], ly[NR], lz[NR];
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-        const int j = j0 + r;
-        // lanes beyond the row still take part in the shuffles below
-        const bool act0 = j < Ny && k0 < g.Nx;
-        p[r] = act0 ? (i * Ny + j) * px + k0 : 0;
-        const int ly0 = GEN ? slab_local(PY, j, false) : -1;
+    const int lz0 = GEN ? slab_local(PZ, i + PZ.off, true) : -1;
+    // lanes beyond the row still take part in the shuffles of the finish phase
+    const bool act0 = j < Ny && k0 < g.Nx;
+    t.p = act0 ? (i * Ny + j) * px + k0 : 0;
+    const int ly0 = GEN ? slab_local(PY, j, false) : -1;
 #ifdef FDTD_BOUNDS_CHECK
-        // a lane whose indices fall outside their arrays records the site and skips
-        act[r] = act0 && vecb::h_fields_ok(g, i, j, k0, lane, p[r]);
-        ly[r] = (ly0 >= 0 && act[r] && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
-                                                       (long long)Nz * PY.wsum * px - V + 1, 5)) ? -1 : ly0;
-        lz[r] = (lz0 >= 0 && act[r] && !vecb::in_range(g, (long long)(lz0 * Ny + j) * px + k0, 0,
-                                                       (long long)PZ.wsum * Ny * px - V + 1, 6)) ? -1 : lz0;
+    // a lane whose indices fall outside their arrays records the site and skips
+    t.act = act0 && vecb::h_fields_ok(g, i, j, k0, lane, t.p);
+    t.ly = (ly0 >= 0 && t.act && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
+                                                  (long long)Nz * PY.wsum * px - V + 1, 5)) ? -1 : ly0;
+    t.lz = (lz0 >= 0 && t.act && !vecb::in_range(g, (long long)(lz0 * Ny + j) * px + k0, 0,
+                                                  (long long)PZ.wsum * Ny * px - V + 1, 6)) ? -1 : lz0;
 #else
-        act[r] = act0;
-        ly[r] = ly0;
-        lz[r] = lz0;
+    t.act = act0;
+    t.ly = ly0;
+    t.lz = lz0;
 #endif
-    }
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = GEN && (xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max);
 
-    if (g.pf > 0 && i + g.pf < Nz && xb * 32 * V < g.Nx) {
+    if (g.pf > 0 && i + g.pf < Nz && xb * 32 * V < g.Nx && j < Ny) {
+        const long long q = (long long)(i + g.pf) * g.plane + (long long)j * px + xb * 32 * V;
 #pragma unroll
-        for (int r = 0; r < NR; r++)
-            if (j0 + r < Ny) {
-                const long long q = (long long)(i + g.pf) * g.plane + (long long)(j0 + r) * px + xb * 32 * V;
-#pragma unroll
-                for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
-            }
+        for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
     }
 
     // a served request's state and capture flag, read with the fields
-    int sstate = SERVE_RUN, scap = 0;
-    if (SERVE) { sstate = __ldg(sg->state); scap = __ldg(sg->capture); }
+    t.sstate = SERVE_RUN;
+    t.scap = 0;
+    if (SERVE) { t.sstate = __ldg(sg->state); t.scap = __ldg(sg->capture); }
 
-    // ---- every load of the thread first
-    T ex[NR][V], ey[NR][V], ez[NR][V], exj[NR][V], ezj[NR][V], exi[NR][V], eyi[NR][V];
-    T hx[NR][V], hy[NR][V], hz[NR][V];
-    T py0[NR][V], py1[NR][V], pz0[NR][V], pz1[NR][V], px0[NR][V], px1[NR][V];
-    T ey_n[NR], ez_n[NR];
-    int lxs[NR][V];
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-        const int j = j0 + r;
-        vecb::vzero<T>(ex[r]); vecb::vzero<T>(ey[r]); vecb::vzero<T>(ez[r]); vecb::vzero<T>(exj[r]);
-        vecb::vzero<T>(ezj[r]); vecb::vzero<T>(exi[r]); vecb::vzero<T>(eyi[r]);
-        ey_n[r] = T(0); ez_n[r] = T(0);
-        if (act[r]) {
-            const int q = p[r];
-            vecb::vload<T>(ex[r], f.c[0] + q); vecb::vload<T>(ey[r], f.c[1] + q); vecb::vload<T>(ez[r], f.c[2] + q);
-            // E of row j+1: the next row's own load, or a load of its own for the last row
-            if (r + 1 == NR && j + 1 < Ny) { vecb::vload<T>(exj[r], f.c[0] + q + px); vecb::vload<T>(ezj[r], f.c[2] + q + px); }
-            if (i + 1 < Nz) { vecb::vload<T>(exi[r], f.c[0] + q + Ny * px); vecb::vload<T>(eyi[r], f.c[1] + q + Ny * px); }
-            else if (g.zhi) { vecb::vload<T>(exi[r], g.zhalo[0] + (q - i * Ny * px)); vecb::vload<T>(eyi[r], g.zhalo[1] + (q - i * Ny * px)); }
-            vecb::vload<T>(hx[r], f.c[3] + q); vecb::vload<T>(hy[r], f.c[4] + q); vecb::vload<T>(hz[r], f.c[5] + q);
-            if (lane == 31 && k0 + V < g.Nx) { ey_n[r] = ld(f.c[1] + q + V); ez_n[r] = ld(f.c[2] + q + V); }
-            if (ly[r] >= 0) {
-                const int s = (i * PY.wsum + ly[r]) * px + k0;
-                vecb::vload<T>(py0[r], PY.psi[0] + s); vecb::vload<T>(py1[r], PY.psi[1] + s);
-            }
-            if (lz[r] >= 0) {
-                const int s = (lz[r] * Ny + j) * px + k0;
-                vecb::vload<T>(pz0[r], PZ.psi[0] + s); vecb::vload<T>(pz1[r], PZ.psi[1] + s);
-            }
+    vecb::vzero<T>(t.ex); vecb::vzero<T>(t.ey); vecb::vzero<T>(t.ez); vecb::vzero<T>(t.exj);
+    vecb::vzero<T>(t.ezj); vecb::vzero<T>(t.exi); vecb::vzero<T>(t.eyi);
+    t.ey_n = T(0); t.ez_n = T(0);
+    if (t.act) {
+        const int q = t.p;
+        vecb::vload<T>(t.ex, f.c[0] + q); vecb::vload<T>(t.ey, f.c[1] + q); vecb::vload<T>(t.ez, f.c[2] + q);
+        if (j + 1 < Ny) { vecb::vload<T>(t.exj, f.c[0] + q + px); vecb::vload<T>(t.ezj, f.c[2] + q + px); }
+        if (i + 1 < Nz) { vecb::vload<T>(t.exi, f.c[0] + q + Ny * px); vecb::vload<T>(t.eyi, f.c[1] + q + Ny * px); }
+        else if (g.zhi) { vecb::vload<T>(t.exi, g.zhalo[0] + (q - i * Ny * px)); vecb::vload<T>(t.eyi, g.zhalo[1] + (q - i * Ny * px)); }
+        vecb::vload<T>(t.hx, f.c[3] + q); vecb::vload<T>(t.hy, f.c[4] + q); vecb::vload<T>(t.hz, f.c[5] + q);
+        if (lane == 31 && k0 + V < g.Nx) { t.ey_n = ld(f.c[1] + q + V); t.ez_n = ld(f.c[2] + q + V); }
+        if (t.ly >= 0) {
+            const int s = (i * PY.wsum + t.ly) * px + k0;
+            vecb::vload<T>(t.py0, PY.psi[0] + s); vecb::vload<T>(t.py1, PY.psi[1] + s);
         }
-#pragma unroll
-        for (int e = 0; e < V; e++) lxs[r][e] = -1;
-        if (xw) {
-            const bool xs = act[r] && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
-#pragma unroll
-            for (int e = 0; e < V; e++) {
-                const int k = k0 + e;
-                lxs[r][e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
-#ifdef FDTD_BOUNDS_CHECK
-                if (lxs[r][e] >= 0 && !vecb::in_range(g, (long long)(i * Ny + j) * PX.wsum + lxs[r][e], 0,
-                                                      (long long)Nz * Ny * PX.wsum, 7))
-                    lxs[r][e] = -1;
-#endif
-                if (lxs[r][e] >= 0) {
-                    const int s = (i * Ny + j) * PX.wsum + lxs[r][e];
-                    px0[r][e] = ld(PX.psi[0] + s); px1[r][e] = ld(PX.psi[1] + s);
-                }
-            }
+        if (t.lz >= 0) {
+            const int s = (t.lz * Ny + j) * px + k0;
+            vecb::vload<T>(t.pz0, PZ.psi[0] + s); vecb::vload<T>(t.pz1, PZ.psi[1] + s);
         }
     }
 #pragma unroll
-    for (int r = 0; r + 1 < NR; r++)
-        if (act[r] && j0 + r + 1 < Ny) {
-#pragma unroll
-            for (int e = 0; e < V; e++) { exj[r][e] = ex[r + 1][e]; ezj[r][e] = ez[r + 1][e]; }
-        }
-    T mx[NR][V], my[NR][V], mz[NR][V];
-    const bool mu_arr = g.bHarr[0] != nullptr;
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-        if (mu_arr && act[r]) {
-            vecb::vload<T>(mx[r], g.bHarr[0] + p[r]); vecb::vload<T>(my[r], g.bHarr[1] + p[r]);
-            vecb::vload<T>(mz[r], g.bHarr[2] + p[r]);
-        } else {
-#pragma unroll
-            for (int e = 0; e < V; e++) { mx[r][e] = g.bH[0]; my[r][e] = g.bH[1]; mz[r][e] = g.bH[2]; }
-        }
-    }
-    if (SERVE) {
-        // the whole warp leaves together (one state per request)
-        if (!serve_running(sstate)) return;
-        if (scap == 1 || scap == 2) {
-            T* const* d = sg->snap[scap - 1];
-#pragma unroll
-            for (int r = 0; r < NR; r++)
-                if (act[r]) {
-                    const int q = p[r];
-                    vecb::vstore<T>(d[0] + q, ex[r]); vecb::vstore<T>(d[1] + q, ey[r]); vecb::vstore<T>(d[2] + q, ez[r]);
-                    vecb::vstore<T>(d[3] + q, hx[r]); vecb::vstore<T>(d[4] + q, hy[r]); vecb::vstore<T>(d[5] + q, hz[r]);
-                }
-        }
-    }
-    const bool srcb = GEN && src.n && vecb::sources_touch<T>(src, 3, i, j0, j0 + NR,
-                                                xb * 32 * V, (xb + 1) * 32 * V);
-    double4 st = make_double4(0, 0, 0, 0);
-    if (srcb) st = g.step_tab[*step_ctr + off];
-
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-        const int j = j0 + r;
-        // ---- x neighbour of the last cell: first cell of the next vector
-        {
-            const T a = __shfl_down_sync(FULL, ey[r][0], 1), b = __shfl_down_sync(FULL, ez[r][0], 1);
-            if (lane != 31) { ey_n[r] = a; ez_n[r] = b; }
-        }
-        if (!act[r]) continue;
+    for (int e = 0; e < V; e++) t.lxs[e] = -1;
+    if (xw) {
+        const bool xs = t.act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
 #pragma unroll
         for (int e = 0; e < V; e++) {
-            const T eyx = e + 1 < V ? ey[r][e + 1] : ey_n[r];
-            const T ezx = e + 1 < V ? ez[r][e + 1] : ez_n[r];
-            const T dEzdy = g.ody * (ezj[r][e] - ez[r][e]);
-            const T dEydz = g.odz * (eyi[r][e] - ey[r][e]);
-            const T dExdz = g.odz * (exi[r][e] - ex[r][e]);
-            const T dEzdx = g.odx * (ezx - ez[r][e]);
-            const T dEydx = g.odx * (eyx - ey[r][e]);
-            const T dExdy = g.ody * (exj[r][e] - ex[r][e]);
-            T Hx = hx[r][e] + mx[r][e] * (dEydz - dEzdy);
-            T Hy = hy[r][e] + my[r][e] * (dEzdx - dExdz);
-            T Hz = hz[r][e] + mz[r][e] * (dExdy - dEydx);
-            if (xw && lxs[r][e] >= 0) {
-                const int l = lxs[r][e];
-                const T kv = ld(PX.kinvH + l), bv = ld(PX.bH + l), cv = ld(PX.cH + l);
-                px0[r][e] = cv * dEydx + bv * px0[r][e];
-                px1[r][e] = cv * dEzdx + bv * px1[r][e];
-                Hz = Hz - mz[r][e] * ((px0[r][e] - dEydx) + dEydx * kv);
-                Hy = Hy + my[r][e] * ((px1[r][e] - dEzdx) + dEzdx * kv);
+            const int k = k0 + e;
+            t.lxs[e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
+#ifdef FDTD_BOUNDS_CHECK
+            if (t.lxs[e] >= 0 && !vecb::in_range(g, (long long)(i * Ny + j) * PX.wsum + t.lxs[e], 0,
+                                                 (long long)Nz * Ny * PX.wsum, 7))
+                t.lxs[e] = -1;
+#endif
+            if (t.lxs[e] >= 0) {
+                const int s = (i * Ny + j) * PX.wsum + t.lxs[e];
+                t.px0[e] = ld(PX.psi[0] + s); t.px1[e] = ld(PX.psi[1] + s);
             }
-            if (ly[r] >= 0) {
-                const int l = ly[r];
-                const T kv = ld(PY.kinvH + l), bv = ld(PY.bH + l), cv = ld(PY.cH + l);
-                py0[r][e] = cv * dExdy + bv * py0[r][e];
-                py1[r][e] = cv * dEzdy + bv * py1[r][e];
-                Hz = Hz + mz[r][e] * ((py0[r][e] - dExdy) + dExdy * kv);
-                Hx = Hx - mx[r][e] * ((py1[r][e] - dEzdy) + dEzdy * kv);
-            }
-            if (lz[r] >= 0) {
-                const int l = lz[r];
-                const T kv = ld(PZ.kinvH + l), bv = ld(PZ.bH + l), cv = ld(PZ.cH + l);
-                pz0[r][e] = cv * dExdz + bv * pz0[r][e];
-                pz1[r][e] = cv * dEydz + bv * pz1[r][e];
-                Hx = Hx + mx[r][e] * ((pz1[r][e] - dEydz) + dEydz * kv);
-                Hy = Hy - my[r][e] * ((pz0[r][e] - dExdz) + dExdz * kv);
-            }
-            if (srcb && k0 + e < g.Nx)
-                add_sources<T>(src, i, j, k0 + e, 3, T(st.x), T(st.y), Hx, Hy, Hz, false);
-            hx[r][e] = Hx; hy[r][e] = Hy; hz[r][e] = Hz;
         }
-        const int q = p[r];
-        vecb::vstore<T>(f.c[3] + q, hx[r]); vecb::vstore<T>(f.c[4] + q, hy[r]); vecb::vstore<T>(f.c[5] + q, hz[r]);
-        if (ly[r] >= 0) {
-            const int s = (i * PY.wsum + ly[r]) * px + k0;
-            vecb::vstore<T>(PY.psi[0] + s, py0[r]); vecb::vstore<T>(PY.psi[1] + s, py1[r]);
-        }
-        if (lz[r] >= 0) {
-            const int s = (lz[r] * Ny + j) * px + k0;
-            vecb::vstore<T>(PZ.psi[0] + s, pz0[r]); vecb::vstore<T>(PZ.psi[1] + s, pz1[r]);
-        }
-        if (xw) {
+    }
+    if (g.bHarr[0] != nullptr && t.act) {
+        vecb::vload<T>(t.mx, g.bHarr[0] + t.p); vecb::vload<T>(t.my, g.bHarr[1] + t.p);
+        vecb::vload<T>(t.mz, g.bHarr[2] + t.p);
+    } else {
 #pragma unroll
-            for (int e = 0; e < V; e++)
-                if (lxs[r][e] >= 0) {
-                    const int s = (i * Ny + j) * PX.wsum + lxs[r][e];
-                    PX.psi[0][s] = px0[r][e]; PX.psi[1][s] = px1[r][e];
-                }
-        }
+        for (int e = 0; e < V; e++) { t.mx[e] = g.bH[0]; t.my[e] = g.bH[1]; t.mz[e] = g.bH[2]; }
     }
 }
 
-template <typename T, int NR = 1, bool GEN = true, bool SERVE = false>
-__device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<T>& f,
-                                     const SourceList<T>& src, const long long* step_ctr,
-                                     int off, int i, int j0, int xb, int lane,
-                                     const ServeGate<T>* sg = nullptr) {
+template <typename T, bool GEN = true, bool SERVE = false>
+__device__ __forceinline__ void h_finish(const GridView<T>& g, const Fields<T>& f, const SourceList<T>& src,
+                                         const long long* step_ctr, int off, int i, int j, int xb,
+                                         int lane, const ServeGate<T>* sg, HTask<T>& t) {
     constexpr int V = vecb::V16<T>::N;
     constexpr unsigned FULL = 0xffffffffu;
+    const int k0 = (xb * 32 + lane) * V;
+    const int Ny = g.Ny, px = g.px;
+    const PmlAxis<T>& PX = g.pml[0];
+    const PmlAxis<T>& PY = g.pml[1];
+    const PmlAxis<T>& PZ = g.pml[2];
+    const bool xw = GEN && (xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max);
+    if (SERVE) {
+        // the whole warp leaves together (one state per request)
+        if (!serve_running(t.sstate)) return;
+        if ((t.scap == 1 || t.scap == 2) && t.act) {
+            T* const* d = sg->snap[t.scap - 1];
+            const int q = t.p;
+            vecb::vstore<T>(d[0] + q, t.ex); vecb::vstore<T>(d[1] + q, t.ey); vecb::vstore<T>(d[2] + q, t.ez);
+            vecb::vstore<T>(d[3] + q, t.hx); vecb::vstore<T>(d[4] + q, t.hy); vecb::vstore<T>(d[5] + q, t.hz);
+        }
+    }
+    const bool srcb = GEN && src.n && vecb::sources_touch<T>(src, 3, i, j, j + 1,
+                                                             xb * 32 * V, (xb + 1) * 32 * V);
+    double4 st = make_double4(0, 0, 0, 0);
+    if (srcb) st = g.step_tab[*step_ctr + off];
+
+    // ---- x neighbour of the last cell: first cell of the next vector
+    {
+        const T a = __shfl_down_sync(FULL, t.ey[0], 1), b = __shfl_down_sync(FULL, t.ez[0], 1);
+        if (lane != 31) { t.ey_n = a; t.ez_n = b; }
+    }
+    if (!t.act) return;
+#pragma unroll
+    for (int e = 0; e < V; e++) {
+        const T eyx = e + 1 < V ? t.ey[e + 1] : t.ey_n;
+        const T ezx = e + 1 < V ? t.ez[e + 1] : t.ez_n;
+        const T dEzdy = g.ody * (t.ezj[e] - t.ez[e]);
+        const T dEydz = g.odz * (t.eyi[e] - t.ey[e]);
+        const T dExdz = g.odz * (t.exi[e] - t.ex[e]);
+        const T dEzdx = g.odx * (ezx - t.ez[e]);
+        const T dEydx = g.odx * (eyx - t.ey[e]);
+        const T dExdy = g.ody * (t.exj[e] - t.ex[e]);
+        T Hx = t.hx[e] + t.mx[e] * (dEydz - dEzdy);
+        T Hy = t.hy[e] + t.my[e] * (dEzdx - dExdz);
+        T Hz = t.hz[e] + t.mz[e] * (dExdy - dEydx);
+        if (xw && t.lxs[e] >= 0) {
+            const int l = t.lxs[e];
+            const T kv = ld(PX.kinvH + l), bv = ld(PX.bH + l), cv = ld(PX.cH + l);
+            t.px0[e] = cv * dEydx + bv * t.px0[e];
+            t.px1[e] = cv * dEzdx + bv * t.px1[e];
+            Hz = Hz - t.mz[e] * ((t.px0[e] - dEydx) + dEydx * kv);
+            Hy = Hy + t.my[e] * ((t.px1[e] - dEzdx) + dEzdx * kv);
+        }
+        if (t.ly >= 0) {
+            const int l = t.ly;
+            const T kv = ld(PY.kinvH + l), bv = ld(PY.bH + l), cv = ld(PY.cH + l);
+            t.py0[e] = cv * dExdy + bv * t.py0[e];
+            t.py1[e] = cv * dEzdy + bv * t.py1[e];
+            Hz = Hz + t.mz[e] * ((t.py0[e] - dExdy) + dExdy * kv);
+            Hx = Hx - t.mx[e] * ((t.py1[e] - dEzdy) + dEzdy * kv);
+        }
+        if (t.lz >= 0) {
+            const int l = t.lz;
+            const T kv = ld(PZ.kinvH + l), bv = ld(PZ.bH + l), cv = ld(PZ.cH + l);
+            t.pz0[e] = cv * dExdz + bv * t.pz0[e];
+            t.pz1[e] = cv * dEydz + bv * t.pz1[e];
+            Hx = Hx + t.mx[e] * ((t.pz1[e] - dEydz) + dEydz * kv);
+            Hy = Hy - t.my[e] * ((t.pz0[e] - dExdz) + dExdz * kv);
+        }
+        if (srcb && k0 + e < g.Nx)
+            add_sources<T>(src, i, j, k0 + e, 3, T(st.x), T(st.y), Hx, Hy, Hz, false);
+        t.hx[e] = Hx; t.hy[e] = Hy; t.hz[e] = Hz;
+    }
+    const int q = t.p;
+    vecb::vstore<T>(f.c[3] + q, t.hx); vecb::vstore<T>(f.c[4] + q, t.hy); vecb::vstore<T>(f.c[5] + q, t.hz);
+    if (t.ly >= 0) {
+        const int s = (i * PY.wsum + t.ly) * px + k0;
+        vecb::vstore<T>(PY.psi[0] + s, t.py0); vecb::vstore<T>(PY.psi[1] + s, t.py1);
+    }
+    if (t.lz >= 0) {
+        const int s = (t.lz * Ny + j) * px + k0;
+        vecb::vstore<T>(PZ.psi[0] + s, t.pz0); vecb::vstore<T>(PZ.psi[1] + s, t.pz1);
+    }
+    if (xw) {
+#pragma unroll
+        for (int e = 0; e < V; e++)
+            if (t.lxs[e] >= 0) {
+                const int s = (i * Ny + j) * PX.wsum + t.lxs[e];
+                PX.psi[0][s] = t.px0[e]; PX.psi[1][s] = t.px1[e];
+            }
+    }
+}
+
+template <typename T, bool GEN = true, bool SERVE = false>
+__device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<T>& f,
+                                             const SourceList<T>& src, const long long* step_ctr,
+                                             int off, int i, int j, int xb, int lane,
+                                             const ServeGate<T>* sg = nullptr) {
+    HTask<T> t;
+    h_load<T, GEN, SERVE>(g, f, i, j, xb, lane, sg, t);
+    h_finish<T, GEN, SERVE>(g, f, src, step_ctr, off, i, j, xb, lane, sg, t);
+}
+
+template <typename T>
+struct ETask {
+    static constexpr int V = vecb::V16<T>::N;
+    T hx[V], hy[V], hz[V], hxj[V], hzj[V], hxi[V], hyi[V];
+    T ex[V], ey[V], ez[V], bx[V], by[V], bz[V];
+    T py2[V], py3[V], pz2[V], pz3[V], px2[V], px3[V], ax[V], ay[V], az[V];
+    T hy_p, hz_p;
+    int lxs[V];
+    int p, ly, lz;
+    bool act;
+    int sstate;
+};
+
+template <typename T, bool GEN = true, bool SERVE = false>
+__device__ __forceinline__ void e_load(const GridView<T>& g, const Fields<T>& f, int i, int j, int xb,
+                                       int lane, const ServeGate<T>* sg, ETask<T>& t) {
+    constexpr int V = vecb::V16<T>::N;
     const int m = xb * 32 + lane;
     const int k0 = m * V;
     const int Ny = g.Ny, px = g.px;
     const PmlAxis<T>& PX = g.pml[0];
     const PmlAxis<T>& PY = g.pml[1];
     const PmlAxis<T>& PZ = g.pml[2];
-    const int lz0 = GEN ? slab_local(PZ, i + PZ.off, true) : -1;   // same for every row of the warp
-    bool act[NR];
-    int p[NR], ly[NR], lz[NR];
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-        const int j = j0 + r;
-        const bool act0 = j < Ny && k0 < g.Nx;
-        p[r] = act0 ? (i * Ny + j) * px + k0 : 0;
-        const int ly0 = GEN ? slab_local(PY, j, false) : -1;
+    const int lz0 = GEN ? slab_local(PZ, i + PZ.off, true) : -1;
+    const bool act0 = j < Ny && k0 < g.Nx;
+    t.p = act0 ? (i * Ny + j) * px + k0 : 0;
+    const int ly0 = GEN ? slab_local(PY, j, false) : -1;
 #ifdef FDTD_BOUNDS_CHECK
-        act[r] = act0 && vecb::e_fields_ok(g, i, j, k0, lane, p[r]);
-        ly[r] = (ly0 >= 0 && act[r] && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
-                                                       (long long)g.Nz * PY.wsum * px - V + 1, 15)) ? -1 : ly0;
-        lz[r] = (lz0 >= 0 && act[r] && !vecb::in_range(g, (long long)(lz0 * Ny + j) * px + k0, 0,
-                                                       (long long)PZ.wsum * Ny * px - V + 1, 16)) ? -1 : lz0;
+    t.act = act0 && vecb::e_fields_ok(g, i, j, k0, lane, t.p);
+    t.ly = (ly0 >= 0 && t.act && !vecb::in_range(g, (long long)(i * PY.wsum + ly0) * px + k0, 0,
+                                                  (long long)g.Nz * PY.wsum * px - V + 1, 15)) ? -1 : ly0;
+    t.lz = (lz0 >= 0 && t.act && !vecb::in_range(g, (long long)(lz0 * Ny + j) * px + k0, 0,
+                                                  (long long)PZ.wsum * Ny * px - V + 1, 16)) ? -1 : lz0;
 #else
-        act[r] = act0;
-        ly[r] = ly0;
-        lz[r] = lz0;
+    t.act = act0;
+    t.ly = ly0;
+    t.lz = lz0;
 #endif
-    }
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = GEN && (xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max);
     const bool lossy = g.aE[0] != nullptr;
 
-    if (g.pf > 0 && i + g.pf < g.Nz && xb * 32 * V < g.Nx) {
+    if (g.pf > 0 && i + g.pf < g.Nz && xb * 32 * V < g.Nx && j < Ny) {
+        const long long q = (long long)(i + g.pf) * g.plane + (long long)j * px + xb * 32 * V;
 #pragma unroll
-        for (int r = 0; r < NR; r++)
-            if (j0 + r < Ny) {
-                const long long q = (long long)(i + g.pf) * g.plane + (long long)(j0 + r) * px + xb * 32 * V;
+        for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
 #pragma unroll
-                for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
-#pragma unroll
-                for (int c = 0; c < 3; c++) vecb::l2_prefetch<T>(g.bE[c] + q, lane, px - xb * 32 * V);
-            }
+        for (int c = 0; c < 3; c++) vecb::l2_prefetch<T>(g.bE[c] + q, lane, px - xb * 32 * V);
     }
 
-    int sstate = SERVE_RUN;
-    if (SERVE) sstate = __ldg(sg->state);
+    t.sstate = SERVE_RUN;
+    if (SERVE) t.sstate = __ldg(sg->state);
 
-    // ---- every load of the thread first
-    T hx[NR][V], hy[NR][V], hz[NR][V], hxj[NR][V], hzj[NR][V], hxi[NR][V], hyi[NR][V];
-    T ex[NR][V], ey[NR][V], ez[NR][V], bx[NR][V], by[NR][V], bz[NR][V];
-    T py2[NR][V], py3[NR][V], pz2[NR][V], pz3[NR][V], px2[NR][V], px3[NR][V], ax[NR][V], ay[NR][V], az[NR][V];
-    T hy_p[NR], hz_p[NR];
-    int lxs[NR][V];
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-        const int j = j0 + r;
-        vecb::vzero<T>(hy[r]); vecb::vzero<T>(hz[r]);
-        hy_p[r] = T(0); hz_p[r] = T(0);
-        if (act[r]) {
-            const int q = p[r];
-            vecb::vload<T>(hx[r], f.c[3] + q); vecb::vload<T>(hy[r], f.c[4] + q); vecb::vload<T>(hz[r], f.c[5] + q);
-            vecb::vload<T>(ex[r], f.c[0] + q); vecb::vload<T>(ey[r], f.c[1] + q); vecb::vload<T>(ez[r], f.c[2] + q);
-            vecb::vload<T>(bx[r], g.bE[0] + q); vecb::vload<T>(by[r], g.bE[1] + q); vecb::vload<T>(bz[r], g.bE[2] + q);
-            // H of row j-1: the previous row's own load, or a load of its own for the first row
-            if (r == 0 && j > 0) { vecb::vload<T>(hxj[r], f.c[3] + q - px); vecb::vload<T>(hzj[r], f.c[5] + q - px); }
-            if (i > 0) { vecb::vload<T>(hxi[r], f.c[3] + q - Ny * px); vecb::vload<T>(hyi[r], f.c[4] + q - Ny * px); }
-            else if (g.zlo) { vecb::vload<T>(hxi[r], g.zhalo[2] + q); vecb::vload<T>(hyi[r], g.zhalo[3] + q); }
-            if (lane == 0 && k0 > 0) { hy_p[r] = ld(f.c[4] + q - 1); hz_p[r] = ld(f.c[5] + q - 1); }
-            if (ly[r] >= 0) {
-                const int s = (i * PY.wsum + ly[r]) * px + k0;
-                vecb::vload<T>(py2[r], PY.psi[2] + s); vecb::vload<T>(py3[r], PY.psi[3] + s);
-            }
-            if (lz[r] >= 0) {
-                const int s = (lz[r] * Ny + j) * px + k0;
-                vecb::vload<T>(pz2[r], PZ.psi[2] + s); vecb::vload<T>(pz3[r], PZ.psi[3] + s);
-            }
-            if (lossy) {
-                vecb::vload<T>(ax[r], g.aE[0] + q); vecb::vload<T>(ay[r], g.aE[1] + q); vecb::vload<T>(az[r], g.aE[2] + q);
-            }
+    vecb::vzero<T>(t.hy); vecb::vzero<T>(t.hz);
+    t.hy_p = T(0); t.hz_p = T(0);
+    if (t.act) {
+        const int q = t.p;
+        vecb::vload<T>(t.hx, f.c[3] + q); vecb::vload<T>(t.hy, f.c[4] + q); vecb::vload<T>(t.hz, f.c[5] + q);
+        vecb::vload<T>(t.ex, f.c[0] + q); vecb::vload<T>(t.ey, f.c[1] + q); vecb::vload<T>(t.ez, f.c[2] + q);
+        vecb::vload<T>(t.bx, g.bE[0] + q); vecb::vload<T>(t.by, g.bE[1] + q); vecb::vload<T>(t.bz, g.bE[2] + q);
+        if (j > 0) { vecb::vload<T>(t.hxj, f.c[3] + q - px); vecb::vload<T>(t.hzj, f.c[5] + q - px); }
+        if (i > 0) { vecb::vload<T>(t.hxi, f.c[3] + q - Ny * px); vecb::vload<T>(t.hyi, f.c[4] + q - Ny * px); }
+        else if (g.zlo) { vecb::vload<T>(t.hxi, g.zhalo[2] + q); vecb::vload<T>(t.hyi, g.zhalo[3] + q); }
+        if (lane == 0 && k0 > 0) { t.hy_p = ld(f.c[4] + q - 1); t.hz_p = ld(f.c[5] + q - 1); }
+        if (t.ly >= 0) {
+            const int s = (i * PY.wsum + t.ly) * px + k0;
+            vecb::vload<T>(t.py2, PY.psi[2] + s); vecb::vload<T>(t.py3, PY.psi[3] + s);
         }
+        if (t.lz >= 0) {
+            const int s = (t.lz * Ny + j) * px + k0;
+            vecb::vload<T>(t.pz2, PZ.psi[2] + s); vecb::vload<T>(t.pz3, PZ.psi[3] + s);
+        }
+        if (lossy) {
+            vecb::vload<T>(t.ax, g.aE[0] + q); vecb::vload<T>(t.ay, g.aE[1] + q); vecb::vload<T>(t.az, g.aE[2] + q);
+        }
+    }
 #pragma unroll
-        for (int e = 0; e < V; e++) lxs[r][e] = -1;
-        if (xw) {
-            const bool xs = act[r] && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
+    for (int e = 0; e < V; e++) t.lxs[e] = -1;
+    if (xw) {
+        const bool xs = t.act && (k0 < PX.w0 || k0 + V - 1 >= PX.edge_max);
 #pragma unroll
-            for (int e = 0; e < V; e++) {
-                const int k = k0 + e;
-                lxs[r][e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
+        for (int e = 0; e < V; e++) {
+            const int k = k0 + e;
+            t.lxs[e] = (xs && k < g.Nx) ? slab_local(PX, k, false) : -1;
 #ifdef FDTD_BOUNDS_CHECK
-                if (lxs[r][e] >= 0 && !vecb::in_range(g, (long long)(i * Ny + j) * PX.wsum + lxs[r][e], 0,
-                                                      (long long)g.Nz * Ny * PX.wsum, 17))
-                    lxs[r][e] = -1;
+            if (t.lxs[e] >= 0 && !vecb::in_range(g, (long long)(i * Ny + j) * PX.wsum + t.lxs[e], 0,
+                                                 (long long)g.Nz * Ny * PX.wsum, 17))
+                t.lxs[e] = -1;
 #endif
-                if (lxs[r][e] >= 0) {
-                    const int s = (i * Ny + j) * PX.wsum + lxs[r][e];
-                    px2[r][e] = ld(PX.psi[2] + s); px3[r][e] = ld(PX.psi[3] + s);
-                }
+            if (t.lxs[e] >= 0) {
+                const int s = (i * Ny + j) * PX.wsum + t.lxs[e];
+                t.px2[e] = ld(PX.psi[2] + s); t.px3[e] = ld(PX.psi[3] + s);
             }
         }
     }
-#pragma unroll
-    for (int r = 1; r < NR; r++)
-        if (act[r]) {
-#pragma unroll
-            for (int e = 0; e < V; e++) { hxj[r][e] = hx[r - 1][e]; hzj[r][e] = hz[r - 1][e]; }
-        }
-    if (SERVE && !serve_running(sstate)) return;   // the whole warp leaves together
-    const bool srcb = GEN && src.n && vecb::sources_touch<T>(src, 0, i, j0, j0 + NR,
-                                                xb * 32 * V, (xb + 1) * 32 * V);
+}
+
+template <typename T, bool GEN = true, bool SERVE = false>
+__device__ __forceinline__ void e_finish(const GridView<T>& g, const Fields<T>& f, const SourceList<T>& src,
+                                         const long long* step_ctr, int off, int i, int j, int xb,
+                                         int lane, ETask<T>& t) {
+    constexpr int V = vecb::V16<T>::N;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int k0 = (xb * 32 + lane) * V;
+    const int Ny = g.Ny, px = g.px;
+    const PmlAxis<T>& PX = g.pml[0];
+    const PmlAxis<T>& PY = g.pml[1];
+    const PmlAxis<T>& PZ = g.pml[2];
+    const bool xw = GEN && (xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max);
+    const bool lossy = g.aE[0] != nullptr;
+    if (SERVE && !serve_running(t.sstate)) return;   // the whole warp leaves together
+    const bool srcb = GEN && src.n && vecb::sources_touch<T>(src, 0, i, j, j + 1,
+                                                             xb * 32 * V, (xb + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_ctr + off];
 
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-        const int j = j0 + r;
-        // ---- x neighbour of the first cell: last cell of the previous vector
-        {
-            const T a = __shfl_up_sync(FULL, hy[r][V - 1], 1), b = __shfl_up_sync(FULL, hz[r][V - 1], 1);
-            if (lane != 0) { hy_p[r] = a; hz_p[r] = b; }
-        }
-        if (!act[r]) continue;
-        if (k0 == 0) { hy_p[r] = h_min_ghost<T>(g.bc[0], hy[r][0], T(0)); hz_p[r] = h_min_ghost<T>(g.bc[0], hz[r][0], T(0)); }
-        if (j == 0) {
-#pragma unroll
-            for (int e = 0; e < V; e++) {
-                hxj[r][e] = h_min_ghost<T>(g.bc[1], hx[r][e], T(0));
-                hzj[r][e] = h_min_ghost<T>(g.bc[1], hz[r][e], T(0));
-            }
-        }
-        if (i == 0 && !g.zlo) {
-#pragma unroll
-            for (int e = 0; e < V; e++) {
-                hxi[r][e] = h_min_ghost<T>(g.bc[2], hx[r][e], T(0));
-                hyi[r][e] = h_min_ghost<T>(g.bc[2], hy[r][e], T(0));
-            }
-        }
+    // ---- x neighbour of the first cell: last cell of the previous vector
+    {
+        const T a = __shfl_up_sync(FULL, t.hy[V - 1], 1), b = __shfl_up_sync(FULL, t.hz[V - 1], 1);
+        if (lane != 0) { t.hy_p = a; t.hz_p = b; }
+    }
+    if (!t.act) return;
+    if (k0 == 0) { t.hy_p = h_min_ghost<T>(g.bc[0], t.hy[0], T(0)); t.hz_p = h_min_ghost<T>(g.bc[0], t.hz[0], T(0)); }
+    if (j == 0) {
 #pragma unroll
         for (int e = 0; e < V; e++) {
-            const T hyx = e > 0 ? hy[r][e - 1] : hy_p[r];
-            const T hzx = e > 0 ? hz[r][e - 1] : hz_p[r];
-            const T dHzdy = g.ody * (hz[r][e] - hzj[r][e]);
-            const T dHydz = g.odz * (hy[r][e] - hyi[r][e]);
-            const T dHxdz = g.odz * (hx[r][e] - hxi[r][e]);
-            const T dHzdx = g.odx * (hz[r][e] - hzx);
-            const T dHydx = g.odx * (hy[r][e] - hyx);
-            const T dHxdy = g.ody * (hx[r][e] - hxj[r][e]);
-            T Ex, Ey, Ez;
-            if (lossy) {
-                Ex = ax[r][e] * ex[r][e] + (dHzdy - dHydz) * bx[r][e];
-                Ey = ay[r][e] * ey[r][e] + (dHxdz - dHzdx) * by[r][e];
-                Ez = az[r][e] * ez[r][e] + (dHydx - dHxdy) * bz[r][e];
-            } else {
-                Ex = ex[r][e] + (dHzdy - dHydz) * bx[r][e];
-                Ey = ey[r][e] + (dHxdz - dHzdx) * by[r][e];
-                Ez = ez[r][e] + (dHydx - dHxdy) * bz[r][e];
-            }
-            if (xw && lxs[r][e] >= 0) {
-                const int l = lxs[r][e];
-                const T kv = ld(PX.kinvE + l), bv = ld(PX.bE + l), cv = ld(PX.cE + l);
-                px2[r][e] = cv * dHydx + bv * px2[r][e];
-                px3[r][e] = cv * dHzdx + bv * px3[r][e];
-                Ez = Ez + ((px2[r][e] - dHydx) + dHydx * kv) * bz[r][e];
-                Ey = Ey - ((px3[r][e] - dHzdx) + dHzdx * kv) * by[r][e];
-            }
-            if (ly[r] >= 0) {
-                const int l = ly[r];
-                const T kv = ld(PY.kinvE + l), bv = ld(PY.bE + l), cv = ld(PY.cE + l);
-                py2[r][e] = cv * dHxdy + bv * py2[r][e];
-                py3[r][e] = cv * dHzdy + bv * py3[r][e];
-                Ez = Ez - ((py2[r][e] - dHxdy) + dHxdy * kv) * bz[r][e];
-                Ex = Ex + ((py3[r][e] - dHzdy) + dHzdy * kv) * bx[r][e];
-            }
-            if (lz[r] >= 0) {
-                const int l = lz[r];
-                const T kv = ld(PZ.kinvE + l), bv = ld(PZ.bE + l), cv = ld(PZ.cE + l);
-                pz2[r][e] = cv * dHxdz + bv * pz2[r][e];
-                pz3[r][e] = cv * dHydz + bv * pz3[r][e];
-                Ex = Ex - ((pz3[r][e] - dHydz) + dHydz * kv) * bx[r][e];
-                Ey = Ey + ((pz2[r][e] - dHxdz) + dHxdz * kv) * by[r][e];
-            }
-            if (srcb && k0 + e < g.Nx)
-                add_sources<T>(src, i, j, k0 + e, 0, T(st.z), T(st.w), Ex, Ey, Ez, true);
-            ex[r][e] = Ex; ey[r][e] = Ey; ez[r][e] = Ez;
-        }
-        const int q = p[r];
-        vecb::vstore<T>(f.c[0] + q, ex[r]); vecb::vstore<T>(f.c[1] + q, ey[r]); vecb::vstore<T>(f.c[2] + q, ez[r]);
-        if (ly[r] >= 0) {
-            const int s = (i * PY.wsum + ly[r]) * px + k0;
-            vecb::vstore<T>(PY.psi[2] + s, py2[r]); vecb::vstore<T>(PY.psi[3] + s, py3[r]);
-        }
-        if (lz[r] >= 0) {
-            const int s = (lz[r] * Ny + j) * px + k0;
-            vecb::vstore<T>(PZ.psi[2] + s, pz2[r]); vecb::vstore<T>(PZ.psi[3] + s, pz3[r]);
-        }
-        if (xw) {
-#pragma unroll
-            for (int e = 0; e < V; e++)
-                if (lxs[r][e] >= 0) {
-                    const int s = (i * Ny + j) * PX.wsum + lxs[r][e];
-                    PX.psi[2][s] = px2[r][e]; PX.psi[3][s] = px3[r][e];
-                }
+            t.hxj[e] = h_min_ghost<T>(g.bc[1], t.hx[e], T(0));
+            t.hzj[e] = h_min_ghost<T>(g.bc[1], t.hz[e], T(0));
         }
     }
+    if (i == 0 && !g.zlo) {
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            t.hxi[e] = h_min_ghost<T>(g.bc[2], t.hx[e], T(0));
+            t.hyi[e] = h_min_ghost<T>(g.bc[2], t.hy[e], T(0));
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < V; e++) {
+        const T hyx = e > 0 ? t.hy[e - 1] : t.hy_p;
+        const T hzx = e > 0 ? t.hz[e - 1] : t.hz_p;
+        const T dHzdy = g.ody * (t.hz[e] - t.hzj[e]);
+        const T dHydz = g.odz * (t.hy[e] - t.hyi[e]);
+        const T dHxdz = g.odz * (t.hx[e] - t.hxi[e]);
+        const T dHzdx = g.odx * (t.hz[e] - hzx);
+        const T dHydx = g.odx * (t.hy[e] - hyx);
+        const T dHxdy = g.ody * (t.hx[e] - t.hxj[e]);
+        T Ex, Ey, Ez;
+        if (lossy) {
+            Ex = t.ax[e] * t.ex[e] + (dHzdy - dHydz) * t.bx[e];
+            Ey = t.ay[e] * t.ey[e] + (dHxdz - dHzdx) * t.by[e];
+            Ez = t.az[e] * t.ez[e] + (dHydx - dHxdy) * t.bz[e];
+        } else {
+            Ex = t.ex[e] + (dHzdy - dHydz) * t.bx[e];
+            Ey = t.ey[e] + (dHxdz - dHzdx) * t.by[e];
+            Ez = t.ez[e] + (dHydx - dHxdy) * t.bz[e];
+        }
+        if (xw && t.lxs[e] >= 0) {
+            const int l = t.lxs[e];
+            const T kv = ld(PX.kinvE + l), bv = ld(PX.bE + l), cv = ld(PX.cE + l);
+            t.px2[e] = cv * dHydx + bv * t.px2[e];
+            t.px3[e] = cv * dHzdx + bv * t.px3[e];
+            Ez = Ez + ((t.px2[e] - dHydx) + dHydx * kv) * t.bz[e];
+            Ey = Ey - ((t.px3[e] - dHzdx) + dHzdx * kv) * t.by[e];
+        }
+        if (t.ly >= 0) {
+            const int l = t.ly;
+            const T kv = ld(PY.kinvE + l), bv = ld(PY.bE + l), cv = ld(PY.cE + l);
+            t.py2[e] = cv * dHxdy + bv * t.py2[e];
+            t.py3[e] = cv * dHzdy + bv * t.py3[e];
+            Ez = Ez - ((t.py2[e] - dHxdy) + dHxdy * kv) * t.bz[e];
+            Ex = Ex + ((t.py3[e] - dHzdy) + dHzdy * kv) * t.bx[e];
+        }
+        if (t.lz >= 0) {
+            const int l = t.lz;
+            const T kv = ld(PZ.kinvE + l), bv = ld(PZ.bE + l), cv = ld(PZ.cE + l);
+            t.pz2[e] = cv * dHxdz + bv * t.pz2[e];
+            t.pz3[e] = cv * dHydz + bv * t.pz3[e];
+            Ex = Ex - ((t.pz3[e] - dHydz) + dHydz * kv) * t.bx[e];
+            Ey = Ey + ((t.pz2[e] - dHxdz) + dHxdz * kv) * t.by[e];
+        }
+        if (srcb && k0 + e < g.Nx)
+            add_sources<T>(src, i, j, k0 + e, 0, T(st.z), T(st.w), Ex, Ey, Ez, true);
+        t.ex[e] = Ex; t.ey[e] = Ey; t.ez[e] = Ez;
+    }
+    const int q = t.p;
+    vecb::vstore<T>(f.c[0] + q, t.ex); vecb::vstore<T>(f.c[1] + q, t.ey); vecb::vstore<T>(f.c[2] + q, t.ez);
+    if (t.ly >= 0) {
+        const int s = (i * PY.wsum + t.ly) * px + k0;
+        vecb::vstore<T>(PY.psi[2] + s, t.py2); vecb::vstore<T>(PY.psi[3] + s, t.py3);
+    }
+    if (t.lz >= 0) {
+        const int s = (t.lz * Ny + j) * px + k0;
+        vecb::vstore<T>(PZ.psi[2] + s, t.pz2); vecb::vstore<T>(PZ.psi[3] + s, t.pz3);
+    }
+    if (xw) {
+#pragma unroll
+        for (int e = 0; e < V; e++)
+            if (t.lxs[e] >= 0) {
+                const int s = (i * Ny + j) * PX.wsum + t.lxs[e];
+                PX.psi[2][s] = t.px2[e]; PX.psi[3][s] = t.px3[e];
+            }
+    }
+}
+
+template <typename T, bool GEN = true, bool SERVE = false>
+__device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<T>& f,
+                                             const SourceList<T>& src, const long long* step_ctr,
+                                             int off, int i, int j, int xb, int lane,
+                                             const ServeGate<T>* sg = nullptr) {
+    ETask<T> t;
+    e_load<T, GEN, SERVE>(g, f, i, j, xb, lane, sg, t);
+    e_finish<T, GEN, SERVE>(g, f, src, step_ctr, off, i, j, xb, lane, t);
 }
 
 }  // namespace fdtdb
