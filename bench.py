@@ -58,6 +58,9 @@ def parse_args():
     ap.add_argument("--copy-halo", action="store_true",
                     help="zslab on one process: exchange halo planes by device copies instead of "
                          "reading the neighbouring slabs' planes in place")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="zslab on one process: launch every step from the host instead of replaying "
+                         "one captured step")
     ap.add_argument("--overlap", action="store_true",
                     help="zslab on one process: halo copies on a side stream, half steps split around "
                          "them (the schedule of the NCCL transport)")
@@ -590,7 +593,8 @@ def run_zslab(args):
     torch.cuda.set_device(local)
     ss = zslab.SlabSet(p, ranges, precision=args.precision, devices=[local],
                        rank=rank if world > 1 else None, overlap=args.overlap,
-                       direct=False if args.copy_halo else None)
+                       direct=False if args.copy_halo else None,
+                       graphs=False if args.host_loop else None)
     times, res = [], None
     with ClockSampler(local) as clk:
         for it in range(args.warmup + args.steps):
@@ -619,7 +623,8 @@ def run_zslab(args):
                    "time_steps_per_solve": res.steps, "n_main": res.n_main,
                    "transport": "nccl" if world > 1 else
                    ("neighbour planes read in place (one GPU)" if ss.direct else "device copies (one GPU)"),
-                   "schedule": "overlapped" if world > 1 or args.overlap else "plain"},
+                   "schedule": "overlapped" if world > 1 or args.overlap else "plain",
+                   "step_graph": ss.graphs},
         "step_us": 1e6 * t / res.steps,
         "clocks": clk.summary(),
     }

@@ -304,6 +304,18 @@ extern "C" int FDTD_slab_step_part(FDTDHandle* h, long long n, int half, int par
                               : slab_step_impl<double>(h, n, half, part);
 }
 
+// The half steps read the step table at (device step base) + n; the base is
+// 0 except while a caller replays steps captured with n = 0 .. K - 1 (a CUDA
+// graph): it then sets the base to the first step of the replay.
+extern "C" int FDTD_slab_set_step(FDTDHandle* h, long long base) {
+    if (!slab_ready(h) || base < 0 || base >= (1LL << 31))
+        return h ? h->fail(FDTD_ERR_ARG, "FDTD_slab_set_step: no slab begun, or bad step") : FDTD_ERR_ARG;
+    long long* sb = h->precision == 32 ? dptr<long long>(h->r32.stepbase) : dptr<long long>(h->r64.stepbase);
+    fdtdb::launch_set_ll(sb, base, h->stream);
+    CK(cudaGetLastError());
+    return FDTD_OK;
+}
+
 extern "C" int FDTD_slab_set_halo_source(FDTDHandle* h, void* const* ptrs) {
     if (!h || !ptrs) return h ? h->fail(FDTD_ERR_ARG, "FDTD_slab_set_halo_source: null argument") : FDTD_ERR_ARG;
     if (!h->slab) return h->fail(FDTD_ERR_ARG, "FDTD_slab_set_halo_source: not a slab (FDTD_slab_set)");

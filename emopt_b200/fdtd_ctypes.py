@@ -181,6 +181,8 @@ libFDTD.FDTD_slab_halo.argtypes = [c_void_p, POINTER(c_void_p), POINTER(c_longlo
 libFDTD.FDTD_slab_halo.restype = c_int
 libFDTD.FDTD_slab_set_halo_source.argtypes = [c_void_p, POINTER(c_void_p)]
 libFDTD.FDTD_slab_set_halo_source.restype = c_int
+libFDTD.FDTD_slab_set_step.argtypes = [c_void_p, c_longlong]
+libFDTD.FDTD_slab_set_step.restype = c_int
 libFDTD.FDTD_slab_sample.argtypes = [c_void_p, POINTER(c_void_p)]
 libFDTD.FDTD_slab_sample.restype = c_int
 libFDTD.FDTD_slab_probe.argtypes = [c_void_p, c_longlong, POINTER(c_double), POINTER(c_double)]
@@ -257,7 +259,7 @@ ADDED_SYMBOLS = ("FDTD_delete", "FDTD_last_error", "FDTD_set_device", "FDTD_set_
                  "FDTD_serve_last_error", "FDTD_serve_admit", "FDTD_serve_advance",
                  "FDTD_serve_finished", "FDTD_serve_collect", "FDTD_serve_info",
                  "FDTD_serve_delete", "FDTD_set_stream", "FDTD_slab_set", "FDTD_slab_begin",
-                 "FDTD_slab_step", "FDTD_slab_step_part", "FDTD_slab_halo", "FDTD_slab_set_halo_source", "FDTD_slab_sample", "FDTD_slab_probe",
+                 "FDTD_slab_step", "FDTD_slab_step_part", "FDTD_slab_halo", "FDTD_slab_set_halo_source", "FDTD_slab_set_step", "FDTD_slab_sample", "FDTD_slab_probe",
                  "FDTD_slab_capture", "FDTD_slab_finish", "FDTD_structured_values",
                  "FDTD_host_register", "FDTD_host_unregister", "FDTD_mode_last_error",
                  "FDTD_mode_assemble", "FDTD_mode_bmul", "FDTD_mode_lines_gemv", "FDTD_mode_couple",

@@ -208,6 +208,15 @@ class CudaSlab:
     def half_step(self, n: int, half: int):
         self._ok(libFDTD.FDTD_slab_step(self.h, n, half), "FDTD_slab_step")
 
+    def set_step(self, base: int):
+        """Device step base of the half steps (FDTD_slab_set_step)."""
+        self._ok(libFDTD.FDTD_slab_set_step(self.h, int(base)), "FDTD_slab_set_step")
+
+    def use_stream(self, stream):
+        """Launch on ``stream`` (a CUDA stream handle) until told otherwise;
+        the slab's own stream is ``self.stream``."""
+        self._ok(libFDTD.FDTD_set_stream(self.h, ctypes.c_void_p(stream)), "FDTD_set_stream")
+
     def half_step_part(self, n: int, half: int, part: int):
         """Part 1: the planes that read no halo plane; part 2: the plane next to
         the neighbour's halo (FDTD_slab_step_part)."""
@@ -251,16 +260,25 @@ class LocalLink:
     stream of the receiving device, after everything queued so far on the
     sending slab's stream, and the receiving slab's stream waits for it only
     before the plane that reads the halo; the half steps run in two parts
-    around it like the NCCL transport's."""
+    around it like the NCCL transport's.  With ``graphs`` (one device and one
+    stream, plain schedule) the steps between two probes are captured once as
+    a CUDA graph and replayed from the slabs' device step base."""
 
-    def __init__(self, slabs, overlap=False, direct=False):
+    def __init__(self, slabs, overlap=False, direct=False, graphs=False):
+        one_stream = (not (direct or graphs)) or len({(s.device, s.stream) for s in slabs}) == 1
         if direct and overlap:
             raise ValueError("direct halo reads need no exchange to overlap")
-        if direct and len({(s.device, s.stream) for s in slabs}) > 1:
+        if direct and not one_stream:
             raise ValueError("direct halo reads need all slabs on one device and one stream")
+        if graphs and (overlap or not one_stream):
+            raise ValueError("graph replays need the plain schedule on one device and one stream")
         self.slabs = slabs
         self.direct = bool(direct)
         self.overlap = bool(overlap)
+        # graphs: run() replays one captured time step of every slab (kernels
+        # and copies) instead of launching from the host step by step
+        self.graphs = bool(graphs)
+        self._graphs = {}
         self._sides = {}
         self._streams = {}
         self._pending = {"E": [], "H": []}
@@ -268,22 +286,77 @@ class LocalLink:
             raise ValueError("overlapped device copies need the slabs' streams")
 
     def _stream(self, slab):
+        """The torch stream object of the stream the slab's library calls
+        run on.  Handle 0 is the device's legacy default stream:
+        ``torch.cuda.ExternalStream(0)`` does not stand for it, so it is taken
+        from ``torch.cuda.default_stream``."""
         st = self._streams.get(id(slab))
         if st is None:
             import torch
-            st = self._streams[id(slab)] = torch.cuda.ExternalStream(
-                slab.stream, device=torch.device("cuda", slab.device))
+            dev = torch.device("cuda", slab.device)
+            st = (torch.cuda.default_stream(dev) if not slab.stream
+                  else torch.cuda.ExternalStream(slab.stream, device=dev))
+            if st.cuda_stream != (slab.stream or 0):
+                raise RuntimeError("no torch stream object for the slab's stream")
+            self._streams[id(slab)] = st
         return st
 
     def attach(self):
-        """Direct mode: point every slab at its neighbours' boundary planes
-        (after every slab's begin, which places its arrays)."""
+        """After every slab's begin (which places its arrays): drop the
+        captured step; in direct mode point every slab at its neighbours'
+        boundary planes."""
+        self._graphs = {}
         if not self.direct:
             return
         for q, s in enumerate(self.slabs):
             above = self.slabs[q + 1].halo["E_send"] if q + 1 < len(self.slabs) else None
             below = self.slabs[q - 1].halo["H_send"] if q > 0 else None
             s.set_halo_source(above, below)
+
+    def _steps_graph(self, count):
+        """``count`` time steps of every slab captured as one CUDA graph (per
+        step: the E exchange, every H half step, the H exchange, every E half
+        step), the half steps captured with n = 0 .. count - 1 relative to the
+        slabs' device step base."""
+        g = self._graphs.get(count)
+        if g is None:
+            import torch
+            s0 = self.slabs[0]
+            main = self._stream(s0)
+            cap = torch.cuda.Stream(device=torch.device("cuda", s0.device))
+            cap.wait_stream(main)
+            g = torch.cuda.CUDAGraph()
+            for s in self.slabs:
+                s.use_stream(cap.cuda_stream)
+            try:
+                with torch.cuda.graph(g, stream=cap):
+                    for m in range(count):
+                        self.exchange_E()
+                        for s in self.slabs:
+                            s.half_step(m, 0)
+                        self.exchange_H()
+                        for s in self.slabs:
+                            s.half_step(m, 1)
+            finally:
+                for s in self.slabs:
+                    s.use_stream(s.stream)
+            main.wait_stream(cap)
+            self._graphs[count] = g
+        return g
+
+    def steps(self, n, count):
+        """Steps n .. n + count - 1 of every slab as one graph replay (one
+        graph per distinct count: the probe period, the tail run)."""
+        if count <= 0:
+            return
+        import torch
+        g = self._steps_graph(count)
+        for s in self.slabs:
+            s.set_step(n)
+        with torch.cuda.stream(self._stream(self.slabs[0])):
+            g.replay()
+        for s in self.slabs:
+            s.set_step(0)
 
     def _start(self, which, pairs):
         """pairs: (receiving slab, destination, sending slab, source)."""
@@ -459,6 +532,8 @@ def run(slabs, link, Tn: int, rtol: float, Nmax: float, fixed_steps: int | None 
                 link.start_E()
 
     steps = steps_overlapped if getattr(link, "overlap", False) else steps_plain
+    if getattr(link, "graphs", False):
+        steps = link.steps
 
     def probe(n_last):
         link.sum_samples([s.sample() for s in slabs])
@@ -510,7 +585,7 @@ class SlabSet:
     """
 
     def __init__(self, p, ranges, precision="fp32", devices=None, link=None, rank=None,
-                 stream=None, t0_device=False, overlap=False, direct=None):
+                 stream=None, t0_device=False, overlap=False, direct=None, graphs=None):
         prm = derive_parameters(p.X, p.Y, p.Z, p.dx, p.dy, p.dz, p.wavelength, 1.0, p.nconv or 10)
         Nx, Ny, Nz = prm["Nx"], prm["Ny"], prm["Nz"]
         self.p = p
@@ -546,13 +621,19 @@ class SlabSet:
             direct = (rank is None and not overlap and len(self.slabs) > 1 and
                       len({(s.device, s.stream) for s in self.slabs}) == 1)
         self.direct = bool(direct)
+        # ... and replay one captured step (CUDA graph) on one device and stream
+        if graphs is None:
+            graphs = (rank is None and not overlap and
+                      len({(s.device, s.stream) for s in self.slabs}) == 1)
+        self.graphs = bool(graphs)
         self.res = None
 
     def begin(self):
         for s in self.slabs:
             s.begin(self.Tn, self.p.fixed_steps, self.Nmax, self.cells)
         if self.link is None:
-            self.link = (LocalLink(self.slabs, overlap=self.overlap, direct=self.direct)
+            self.link = (LocalLink(self.slabs, overlap=self.overlap, direct=self.direct,
+                                   graphs=self.graphs)
                          if self.rank is None else TorchLink(self.slabs[0]))
         if hasattr(self.link, "attach"):
             self.link.attach()
@@ -610,10 +691,11 @@ def grad_eps_planar(fwd, adj, box, ranges, link, device=0):
 
 
 def solve(p, ranges, precision="fp32", devices=None, link=None, rank=None, stream=None,
-          overlap=False, direct=None):
+          overlap=False, direct=None, graphs=None):
     """Solve problem ``p`` split into the slabs ``ranges`` (see ``SlabSet``).
     Returns (result, {slab index: six complex [I, Ny, Nx] arrays})."""
-    ss = SlabSet(p, ranges, precision, devices, link, rank, stream, overlap=overlap, direct=direct)
+    ss = SlabSet(p, ranges, precision, devices, link, rank, stream, overlap=overlap, direct=direct,
+                 graphs=graphs)
     try:
         ss.begin()
         res = ss.run()

@@ -291,6 +291,13 @@ int FDTD_slab_halo(FDTDHandle *h, void **ptrs, long long *plane_elems);
  * Holds until the next call. */
 int FDTD_slab_set_halo_source(FDTDHandle *h, void *const *ptrs);
 
+/* The half steps read the source table at (device step base) + n.  The base
+ * is 0 after FDTD_slab_begin; FDTD_slab_set_step sets it in stream order, so
+ * that K steps captured once with n = 0 .. K - 1 (a CUDA graph of
+ * FDTD_slab_step calls) replay as steps base .. base + K - 1.  Set it back to
+ * 0 before FDTD_slab_probe. */
+int FDTD_slab_set_step(FDTDHandle *h, long long base);
+
 /* Writes the probe values this slab holds (3 x npoints doubles, zero for the
  * points of other slabs) into a device buffer and returns its address; the
  * caller sums the buffers of all slabs into every slab's buffer. */

@@ -20,7 +20,7 @@ def test_library_exports_header_symbols():
     from emopt_b200 import fdtd_ctypes as ct
     lib = ctypes.CDLL(ct.so_path)
     syms = header_symbols()
-    assert len(syms) == 73
+    assert len(syms) == 74
     for s in syms:
         assert hasattr(lib, s), s
     assert set(ct.REFERENCE_SYMBOLS) | set(ct.ADDED_SYMBOLS) == set(syms)

@@ -39,16 +39,20 @@ def _single(p, precision):
 
 
 def _slabs(p, nslab, precision, mode="direct"):
-    """mode: "direct" (the slabs read each other's boundary planes in place),
-    "copy" (halo planes exchanged by device copies between the half steps) or
-    "overlap" (copies on a side stream, the half steps in two parts around
-    them)."""
+    """mode: "direct" (the slabs read each other's boundary planes in place,
+    one captured time step replayed as a CUDA graph), "direct-loop" (the same
+    launched from the host step by step), "copy" (halo planes exchanged by
+    device copies between the half steps, graph replays) or "overlap" (copies
+    on a side stream, the half steps in two parts around them)."""
     ranges = zslab.ownership(p.shape[0], nslab)
+    direct = mode.startswith("direct")
     ss = zslab.SlabSet(p, ranges, precision=precision, overlap=mode == "overlap",
-                       direct=None if mode == "direct" else False)
+                       direct=None if direct else False,
+                       graphs=False if mode == "direct-loop" else None)
     try:
         ss.begin()
-        assert ss.link.direct == (mode == "direct") and ss.link.overlap == (mode == "overlap")
+        assert ss.link.direct == direct and ss.link.overlap == (mode == "overlap")
+        assert ss.link.graphs == (mode in ("direct", "copy"))
         res = ss.run()
         parts = ss.finish()
     finally:
@@ -57,7 +61,7 @@ def _slabs(p, nslab, precision, mode="direct"):
     return F, res
 
 
-@pytest.mark.parametrize("mode", ["direct", "copy"])
+@pytest.mark.parametrize("mode", ["direct", "direct-loop", "copy"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("name", list(CASES))
 def test_fixed_steps_equal_single_gpu_solve(name, precision, mode):
