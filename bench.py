@@ -50,7 +50,7 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--kernel", default="auto",
-                    choices=["auto", "scalar", "fused", "vector"])
+                    choices=["auto", "scalar", "fused", "vector", "split"])
     ap.add_argument("--workload", default="mmi",
                     choices=["mmi", "waveguide", "serving", "grad", "grating", "zslab", "modes"])
     ap.add_argument("--slabs", type=int, default=2,

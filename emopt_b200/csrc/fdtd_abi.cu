@@ -741,8 +741,9 @@ int FDTD_set_precision(FDTDHandle* h, int bits) {
 }
 
 int FDTD_set_kernel(FDTDHandle* h, int which) {
-    if (which != 0 && which != 1 && which != 3 && which != 5)
-        return h->fail(FDTD_ERR_ARG, "kernel must be 0 (auto), 1 (scalar), 3 (fused) or 5 (vector)");
+    if (which != 0 && which != 1 && which != 3 && which != 5 && which != 6)
+        return h->fail(FDTD_ERR_ARG,
+                       "kernel must be 0 (auto), 1 (scalar), 3 (fused), 5 (vector) or 6 (vector, interior/rim split)");
     h->kernel = which;
     return FDTD_OK;
 }
@@ -1027,12 +1028,24 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
         if (h->bc[a] != '0' && h->bc[a] != 'E' && h->bc[a] != 'H') periodic = true;
     bool small_index = (long long)h->Nz * h->Ny * ((h->Nx + 31) / 32 * 32) < (1LL << 31) &&
                        (long long)h->Nz * h->Ny * (h->w[0] + h->w[1]) < (1LL << 31);
-    // kernel ids: 0 auto (the vector pair), 1 scalar H/E pair, 3 fused
-    // z-marching step, 5 vector H/E pair
-    int kid = h->kernel == 0 ? 5 : h->kernel;
+    // kernel ids: 0 auto, 1 scalar H/E pair, 3 fused z-marching step, 5
+    // vector H/E pair, 6 vector pair split into interior and rim launches.
+    // Auto takes the split pair in float32 when at least 60% of the warp
+    // tasks lie in no CPML slab (the 1201 x 601 x 301 grating slab, 69%:
+    // 3293 instead of 3605 us per step; the 321 x 161 x 101 MMI block, 23%:
+    // 143 instead of 122), else the vector pair.
+    int kid = h->kernel;
+    if (kid == 0) {
+        kid = 5;
+        if (sizeof(T) == 4 && !periodic && small_index) {
+            const fdtdb::GridView<T> gv = make_view<T>(h, r, 0);
+            if (fdtdb::split_interior_fraction<T>(gv) >= 0.6) kid = 6;
+        }
+    }
     if (periodic || !small_index) kid = 1;
     const bool fused = kid == 3;
     const bool vec = kid == 5;
+    const bool split = kid == 6;
     int rc;
     CK(cudaEventRecord(h->ev[2], h->stream));
     if ((rc = alloc_resident<T>(h, r, fused)) != FDTD_OK) return rc;
@@ -1112,6 +1125,8 @@ int solve_impl(FDTDHandle* h, const FDTDSolveOptions* o, FDTDSolveResult* res) {
                                                 odd ? f0 : f1, src, sb, (int)q, zc, h->stream));
             } else if (vec) {
                 CK(fdtdb::launch_step_vec<T>(g0, f0, src, sb, (int)q, h->stream));
+            } else if (split) {
+                CK(fdtdb::launch_step_split<T>(g0, f0, src, sb, (int)q, h->stream));
 
             } else {
                 fdtdb::launch_step_unfused<T>(g0, f0, src, sb, (int)q, h->stream);

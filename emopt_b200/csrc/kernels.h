@@ -18,6 +18,16 @@ template <typename T>
 cudaError_t launch_step_vec(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
                             const long long* step_base, int off, cudaStream_t st);
 
+// The same time step split into an interior launch (no CPML code, multi-warp
+// CTAs) and a rim launch (the CPML slabs) per half step (vec_kernels.cu).
+template <typename T>
+cudaError_t launch_step_split(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
+                              const long long* step_base, int off, cudaStream_t st);
+
+// Fraction of the warp tasks that the interior launch of the split pair takes.
+template <typename T>
+double split_interior_fraction(const GridView<T>& g);
+
 // One half step (half 0: H, 1: E) of the vector pair over planes
 // [i0, i0 + ni): the z slabs of a distributed solve exchange halo planes
 // between the two, and update the planes next to a halo apart from the rest.

@@ -158,8 +158,10 @@ __device__ bool e_fields_ok(const GridView<T>& g, int i, int j, int k0, int lane
 // stores) around a register set of the task (HTask / ETask).  A task writes
 // only its own cells, and no array a half step writes is read by another
 // task of that half step, so tasks may run in any order.
-// GEN = false: the caller guarantees that the task touches no CPML slab and
-// no source box (vecb::plain_warp); the CPML and source code is compiled out.
+// GEN = false: the caller guarantees that the task touches no CPML slab; the
+// CPML code is compiled out, and so is the source code unless SRC is set
+// (default: SRC = GEN; with GEN = false the caller then also guarantees that
+// no source box touches the task, vecb::plain_warp).
 // SERVE: a served request's state gates the stores, and the H half step
 // writes the fields it read into a snapshot set on a capture step
 // (ServeGate).
@@ -266,7 +268,7 @@ __device__ __forceinline__ void h_load(const GridView<T>& g, const Fields<T>& f,
     }
 }
 
-template <typename T, bool GEN = true, bool SERVE = false>
+template <typename T, bool GEN = true, bool SERVE = false, bool SRC = GEN>
 __device__ __forceinline__ void h_finish(const GridView<T>& g, const Fields<T>& f, const SourceList<T>& src,
                                          const long long* step_ctr, int off, int i, int j, int xb,
                                          int lane, const ServeGate<T>* sg, HTask<T>& t) {
@@ -288,7 +290,7 @@ __device__ __forceinline__ void h_finish(const GridView<T>& g, const Fields<T>& 
             vecb::vstore<T>(d[3] + q, t.hx); vecb::vstore<T>(d[4] + q, t.hy); vecb::vstore<T>(d[5] + q, t.hz);
         }
     }
-    const bool srcb = GEN && src.n && vecb::sources_touch<T>(src, 3, i, j, j + 1,
+    const bool srcb = SRC && src.n && vecb::sources_touch<T>(src, 3, i, j, j + 1,
                                                              xb * 32 * V, (xb + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_ctr + off];
@@ -360,14 +362,14 @@ __device__ __forceinline__ void h_finish(const GridView<T>& g, const Fields<T>& 
     }
 }
 
-template <typename T, bool GEN = true, bool SERVE = false>
+template <typename T, bool GEN = true, bool SERVE = false, bool SRC = GEN>
 __device__ __forceinline__ void vec_update_H(const GridView<T>& g, const Fields<T>& f,
                                              const SourceList<T>& src, const long long* step_ctr,
                                              int off, int i, int j, int xb, int lane,
                                              const ServeGate<T>* sg = nullptr) {
     HTask<T> t;
     h_load<T, GEN, SERVE>(g, f, i, j, xb, lane, sg, t);
-    h_finish<T, GEN, SERVE>(g, f, src, step_ctr, off, i, j, xb, lane, sg, t);
+    h_finish<T, GEN, SERVE, SRC>(g, f, src, step_ctr, off, i, j, xb, lane, sg, t);
 }
 
 template <typename T>
@@ -467,7 +469,7 @@ __device__ __forceinline__ void e_load(const GridView<T>& g, const Fields<T>& f,
     }
 }
 
-template <typename T, bool GEN = true, bool SERVE = false>
+template <typename T, bool GEN = true, bool SERVE = false, bool SRC = GEN>
 __device__ __forceinline__ void e_finish(const GridView<T>& g, const Fields<T>& f, const SourceList<T>& src,
                                          const long long* step_ctr, int off, int i, int j, int xb,
                                          int lane, ETask<T>& t) {
@@ -481,7 +483,7 @@ __device__ __forceinline__ void e_finish(const GridView<T>& g, const Fields<T>& 
     const bool xw = GEN && (xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max);
     const bool lossy = g.aE[0] != nullptr;
     if (SERVE && !serve_running(t.sstate)) return;   // the whole warp leaves together
-    const bool srcb = GEN && src.n && vecb::sources_touch<T>(src, 0, i, j, j + 1,
+    const bool srcb = SRC && src.n && vecb::sources_touch<T>(src, 0, i, j, j + 1,
                                                              xb * 32 * V, (xb + 1) * 32 * V);
     double4 st = make_double4(0, 0, 0, 0);
     if (srcb) st = g.step_tab[*step_ctr + off];
@@ -575,14 +577,14 @@ __device__ __forceinline__ void e_finish(const GridView<T>& g, const Fields<T>& 
     }
 }
 
-template <typename T, bool GEN = true, bool SERVE = false>
+template <typename T, bool GEN = true, bool SERVE = false, bool SRC = GEN>
 __device__ __forceinline__ void vec_update_E(const GridView<T>& g, const Fields<T>& f,
                                              const SourceList<T>& src, const long long* step_ctr,
                                              int off, int i, int j, int xb, int lane,
                                              const ServeGate<T>* sg = nullptr) {
     ETask<T> t;
     e_load<T, GEN, SERVE>(g, f, i, j, xb, lane, sg, t);
-    e_finish<T, GEN, SERVE>(g, f, src, step_ctr, off, i, j, xb, lane, t);
+    e_finish<T, GEN, SERVE, SRC>(g, f, src, step_ctr, off, i, j, xb, lane, t);
 }
 
 }  // namespace fdtdb

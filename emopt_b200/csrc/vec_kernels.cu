@@ -10,6 +10,8 @@
 // registers, 16 warps per SM) took 167 us per step in fp32 (216 and 233 at 12
 // and 20 CTAs per SM) and 445 us in fp64: fewer resident warps cost more
 // than the overlap gained.
+#include <algorithm>
+
 #include "kernels.h"
 #include "vec_body.cuh"
 
@@ -47,6 +49,152 @@ k_update_E_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* s
         vec_update_E<T, false>(g, f, src, step_base, off, i, j, blockIdx.x, threadIdx.x);
     else
         vec_update_E<T, true>(g, f, src, step_base, off, i, j, blockIdx.x, threadIdx.x);
+}
+
+// ------------------------------------------------------------- interior/rim
+// The same half steps split by task: the interior box (warp tasks that lie in
+// no CPML slab) runs a body without CPML code, which needs 40-48 registers
+// instead of 64, in multi-warp CTAs (more resident warps per SM); the rim
+// (the tasks of the CPML slabs: whole z-slab planes, then the y-slab rows of
+// the other planes, then the x-slab blocks of the other rows) runs the full
+// body in single-warp CTAs.  Every task belongs to exactly one launch and is
+// computed as by the single kernels, so the fields are the same.
+struct SplitBox {
+    int zi0, zi1, yj0, yj1, xb0, xb1;   // interior box: planes, rows, 64-cell blocks (half open)
+    int nxb, Ny, Nz;
+    long long nz_tasks, ny_tasks;        // rim tasks in the z slabs, in the y slabs
+};
+
+template <typename T>
+bool split_box(const GridView<T>& g, SplitBox& b) {
+    constexpr int W = 32 * vecb::V16<T>::N;   // cells per warp task
+    const PmlAxis<T>& PX = g.pml[0];
+    const PmlAxis<T>& PY = g.pml[1];
+    const PmlAxis<T>& PZ = g.pml[2];
+    b.nxb = ((g.Nx + vecb::V16<T>::N - 1) / vecb::V16<T>::N + 31) / 32;
+    b.Ny = g.Ny;
+    b.Nz = g.Nz;
+    // plane i is in no z slab when w0 <= i + off <= edge_max (slab_local, strict max)
+    b.zi0 = std::max(0, PZ.w0 - PZ.off);
+    b.zi1 = std::min(g.Nz, PZ.edge_max - PZ.off + 1);
+    // row j is in no y slab when w0 <= j < edge_max
+    b.yj0 = PY.w0;
+    b.yj1 = std::min(g.Ny, PY.edge_max);
+    // block xb (cells W xb .. W xb + W - 1) is in no x slab when they lie in [w0, edge_max)
+    b.xb0 = (PX.w0 + W - 1) / W;
+    b.xb1 = std::min(PX.edge_max, g.Nx) / W;
+    if (b.zi1 <= b.zi0 || b.yj1 <= b.yj0 || b.xb1 <= b.xb0) return false;
+    b.nz_tasks = (long long)(g.Nz - (b.zi1 - b.zi0)) * g.Ny * b.nxb;
+    b.ny_tasks = (long long)(b.zi1 - b.zi0) * (g.Ny - (b.yj1 - b.yj0)) * b.nxb;
+    return true;
+}
+
+#ifndef VEC_INT_WARPS
+#define VEC_INT_WARPS 2
+#endif
+#ifndef VEC_INT_MINB32
+#define VEC_INT_MINB32 18
+#endif
+#define VEC_INT_MINB(T) (sizeof(T) == 8 ? 10 : VEC_INT_MINB32)
+
+template <typename T>
+__global__ void __launch_bounds__(32 * VEC_INT_WARPS, VEC_INT_MINB(T))
+k_update_H_int(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
+               SplitBox b) {
+    const int j = b.yj0 + (int)(blockIdx.y * VEC_INT_WARPS + threadIdx.y);
+    if (j >= b.yj1) return;   // the whole warp
+    vec_update_H<T, false, false, true>(g, f, src, step_base, off, b.zi0 + (int)blockIdx.z, j,
+                                        b.xb0 + (int)blockIdx.x, threadIdx.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * VEC_INT_WARPS, VEC_INT_MINB(T))
+k_update_E_int(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
+               SplitBox b) {
+    const int j = b.yj0 + (int)(blockIdx.y * VEC_INT_WARPS + threadIdx.y);
+    if (j >= b.yj1) return;
+    vec_update_E<T, false, false, true>(g, f, src, step_base, off, b.zi0 + (int)blockIdx.z, j,
+                                        b.xb0 + (int)blockIdx.x, threadIdx.x);
+}
+
+// Rim task t -> (plane, row, block).
+__device__ __forceinline__ void rim_task(const SplitBox& b, long long t, int& i, int& j, int& xb) {
+    if (t < b.nz_tasks) {
+        const long long per = (long long)b.Ny * b.nxb;
+        const int p = (int)(t / per);
+        const long long r = t - p * per;
+        i = p < b.zi0 ? p : b.zi1 + (p - b.zi0);
+        j = (int)(r / b.nxb);
+        xb = (int)(r - (long long)j * b.nxb);
+        return;
+    }
+    t -= b.nz_tasks;
+    if (t < b.ny_tasks) {
+        const int rows = b.Ny - (b.yj1 - b.yj0);
+        const long long per = (long long)rows * b.nxb;
+        const int p = (int)(t / per);
+        const long long r = t - p * per;
+        const int q = (int)(r / b.nxb);
+        i = b.zi0 + p;
+        j = q < b.yj0 ? q : b.yj1 + (q - b.yj0);
+        xb = (int)(r - (long long)q * b.nxb);
+        return;
+    }
+    t -= b.ny_tasks;
+    const int blocks = b.nxb - (b.xb1 - b.xb0);
+    const long long per = (long long)(b.yj1 - b.yj0) * blocks;
+    const int p = (int)(t / per);
+    const long long r = t - p * per;
+    const int q = (int)(r / blocks);
+    const int c = (int)(r - (long long)q * blocks);
+    i = b.zi0 + p;
+    j = b.yj0 + q;
+    xb = c < b.xb0 ? c : b.xb1 + (c - b.xb0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(sizeof(T) == 8 ? 32 : 256, VEC_MINB(T))
+k_update_H_rim(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
+               SplitBox b) {
+    int i, j, xb;
+    rim_task(b, blockIdx.x, i, j, xb);
+    vec_update_H<T, true>(g, f, src, step_base, off, i, j, xb, threadIdx.x);
+}
+
+// bounded to 32 resident CTAs in float32 (64 registers; the task decode
+// would take it to 72)
+template <typename T>
+__global__ void __launch_bounds__(32, sizeof(T) == 8 ? 18 : 32)
+k_update_E_rim(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
+               SplitBox b) {
+    int i, j, xb;
+    rim_task(b, blockIdx.x, i, j, xb);
+    vec_update_E<T, true>(g, f, src, step_base, off, i, j, xb, threadIdx.x);
+}
+
+template <typename T>
+double split_interior_fraction(const GridView<T>& g) {
+    SplitBox b;
+    if (!split_box(g, b)) return 0.0;
+    return (double)(b.zi1 - b.zi0) * (b.yj1 - b.yj0) * (b.xb1 - b.xb0) / ((double)b.Nz * b.Ny * b.nxb);
+}
+
+template <typename T>
+cudaError_t launch_step_split(const GridView<T>& g, T* const* fields, const SourceList<T>& src,
+                              const long long* step_base, int off, cudaStream_t st) {
+    SplitBox b;
+    if (!split_box(g, b)) return launch_step_vec<T>(g, fields, src, step_base, off, st);
+    Fields<T> f;
+    for (int c = 0; c < 6; c++) f.c[c] = fields[c];
+    const long long rim = (long long)b.Nz * b.Ny * b.nxb -
+                          (long long)(b.zi1 - b.zi0) * (b.yj1 - b.yj0) * (b.xb1 - b.xb0);
+    dim3 iblock(32, VEC_INT_WARPS);
+    dim3 igrid(b.xb1 - b.xb0, (b.yj1 - b.yj0 + VEC_INT_WARPS - 1) / VEC_INT_WARPS, b.zi1 - b.zi0);
+    k_update_H_int<T><<<igrid, iblock, 0, st>>>(g, f, src, step_base, off, b);
+    if (rim > 0) k_update_H_rim<T><<<(unsigned)rim, 32, 0, st>>>(g, f, src, step_base, off, b);
+    k_update_E_int<T><<<igrid, iblock, 0, st>>>(g, f, src, step_base, off, b);
+    if (rim > 0) k_update_E_rim<T><<<(unsigned)rim, 32, 0, st>>>(g, f, src, step_base, off, b);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ grid
@@ -90,5 +238,13 @@ template cudaError_t launch_step_vec<float>(const GridView<float>&, float* const
 template cudaError_t launch_step_vec<double>(const GridView<double>&, double* const*,
                                              const SourceList<double>&, const long long*, int,
                                              cudaStream_t);
+template double split_interior_fraction<float>(const GridView<float>&);
+template double split_interior_fraction<double>(const GridView<double>&);
+template cudaError_t launch_step_split<float>(const GridView<float>&, float* const*,
+                                              const SourceList<float>&, const long long*, int,
+                                              cudaStream_t);
+template cudaError_t launch_step_split<double>(const GridView<double>&, double* const*,
+                                               const SourceList<double>&, const long long*, int,
+                                               cudaStream_t);
 
 }  // namespace fdtdb

@@ -102,7 +102,7 @@ class FDTD(MaxwellSolver):
     """3D continuous-wave FDTD solver (drop-in for ``emopt.fdtd.FDTD``)."""
 
     # time-stepping kernels of FDTD_solve_cw (include/emopt_fdtd.h, FDTD_set_kernel)
-    KERNELS = {"auto": 0, "scalar": 1, "fused": 3, "vector": 5}
+    KERNELS = {"auto": 0, "scalar": 1, "fused": 3, "vector": 5, "split": 6}
 
     def __init__(self, X, Y, Z, dx, dy, dz, wavelength, rtol=1e-6, nconv=None,
                  min_rindex=1.0, complex_eps=False, dist_method="auto",

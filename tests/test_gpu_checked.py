@@ -19,8 +19,8 @@ from helpers import ROOT
 
 pytestmark = pytest.mark.gpu
 
-SELECT = ("(test_gpu_parity and vector) or every_bc or test_fixed_steps "
-          "or test_gpu_serving")
+SELECT = ("(test_gpu_parity and (vector or split)) or every_bc or test_fixed_steps "
+          "or test_gpu_serving or test_split_pair")
 
 
 def test_parity_cases_pass_with_index_checks():
@@ -28,7 +28,8 @@ def test_parity_cases_pass_with_index_checks():
     assert os.path.exists(lib), "build the checked library first (python -m emopt_b200.build)"
     env = dict(os.environ, EMOPT_B200_LIB=lib)
     cmd = [sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p", "no:cacheprovider",
-           "-k", SELECT, "tests/test_gpu_parity.py", "tests/test_gpu_zslab.py", "tests/test_gpu_serving.py"]
+           "-k", SELECT, "tests/test_gpu_parity.py", "tests/test_gpu_zslab.py", "tests/test_gpu_serving.py",
+           "tests/test_gpu_split.py"]
     out = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=1200)
     print(out.stdout[-3000:], out.stderr[-2000:])
     assert out.returncode == 0

@@ -126,7 +126,7 @@ def test_abi_per_call_field_arrays_match_oracle_each_step():
 
 
 # ------------------------------------------------ device-resident solve
-@pytest.mark.parametrize("kernel", ["fused", "vector", "scalar"])
+@pytest.mark.parametrize("kernel", ["fused", "vector", "split", "scalar"])
 @pytest.mark.parametrize("name", list(BOX_KW))
 def test_solve_cw_fp64_matches_golden(name, kernel):
     g = golden(f"box_{name}.npz")
@@ -156,7 +156,7 @@ def test_solve_cw_fp64_every_bc_matches_oracle(bc, cplx, kernel):
     assert rel_l2(F, np.stack(ref["fields"])) < 1e-11
 
 
-@pytest.mark.parametrize("kernel", ["fused", "vector", "scalar"])
+@pytest.mark.parametrize("kernel", ["fused", "vector", "split", "scalar"])
 @pytest.mark.parametrize("name", list(TAIL_KW))
 def test_row_tail_matches_golden(name, kernel):
     g = golden(f"box_{name}.npz")
@@ -172,7 +172,7 @@ def test_row_tail_matches_golden(name, kernel):
         assert rel_l2(F32, g["fields"]) < 1e-4
 
 
-@pytest.mark.parametrize("kernel", ["fused", "vector", "scalar"])
+@pytest.mark.parametrize("kernel", ["fused", "vector", "split", "scalar"])
 def test_solve_cw_fp64_converging_step_count(kernel):
     """Run to rtol = 1e-6: the step count is bit-for-bit the reference's."""
     g = golden("box_converge.npz")
@@ -215,7 +215,7 @@ def test_solve_cw_waveguide_full_field_vs_oracle():
     assert err32 < 1e-4
 
 
-@pytest.mark.parametrize("kernel", ["fused", "vector", "scalar"])
+@pytest.mark.parametrize("kernel", ["fused", "vector", "split", "scalar"])
 def test_fp32_box_error(kernel):
     g = golden("box_converge.npz")
     p = P.random_box(seed=11, shape=(10, 12, 15), fixed_steps=None, rtol=1e-6)
