@@ -117,36 +117,38 @@ k_update_E_int(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* s
                                         b.xb0 + (int)blockIdx.x, threadIdx.x);
 }
 
-// Rim task t -> (plane, row, block).
-__device__ __forceinline__ void rim_task(const SplitBox& b, long long t, int& i, int& j, int& xb) {
-    if (t < b.nz_tasks) {
-        const long long per = (long long)b.Ny * b.nxb;
-        const int p = (int)(t / per);
-        const long long r = t - p * per;
+// Rim task t -> (plane, row, block), in 32-bit arithmetic: the split pair
+// runs only on grids of fewer than 2^31 cells, so task counts fit.
+__device__ __forceinline__ void rim_task(const SplitBox& b, int t, int& i, int& j, int& xb) {
+    const int nz = (int)b.nz_tasks, ny = (int)b.ny_tasks;
+    if (t < nz) {
+        const int per = b.Ny * b.nxb;
+        const int p = t / per;
+        const int r = t - p * per;
         i = p < b.zi0 ? p : b.zi1 + (p - b.zi0);
-        j = (int)(r / b.nxb);
-        xb = (int)(r - (long long)j * b.nxb);
+        j = r / b.nxb;
+        xb = r - j * b.nxb;
         return;
     }
-    t -= b.nz_tasks;
-    if (t < b.ny_tasks) {
+    t -= nz;
+    if (t < ny) {
         const int rows = b.Ny - (b.yj1 - b.yj0);
-        const long long per = (long long)rows * b.nxb;
-        const int p = (int)(t / per);
-        const long long r = t - p * per;
-        const int q = (int)(r / b.nxb);
+        const int per = rows * b.nxb;
+        const int p = t / per;
+        const int r = t - p * per;
+        const int q = r / b.nxb;
         i = b.zi0 + p;
         j = q < b.yj0 ? q : b.yj1 + (q - b.yj0);
-        xb = (int)(r - (long long)q * b.nxb);
+        xb = r - q * b.nxb;
         return;
     }
-    t -= b.ny_tasks;
+    t -= ny;
     const int blocks = b.nxb - (b.xb1 - b.xb0);
-    const long long per = (long long)(b.yj1 - b.yj0) * blocks;
-    const int p = (int)(t / per);
-    const long long r = t - p * per;
-    const int q = (int)(r / blocks);
-    const int c = (int)(r - (long long)q * blocks);
+    const int per = (b.yj1 - b.yj0) * blocks;
+    const int p = t / per;
+    const int r = t - p * per;
+    const int q = r / blocks;
+    const int c = r - q * blocks;
     i = b.zi0 + p;
     j = b.yj0 + q;
     xb = c < b.xb0 ? c : b.xb1 + (c - b.xb0);
@@ -157,7 +159,7 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 32 : 256, VEC_MINB(T))
 k_update_H_rim(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
                SplitBox b) {
     int i, j, xb;
-    rim_task(b, blockIdx.x, i, j, xb);
+    rim_task(b, (int)blockIdx.x, i, j, xb);
     vec_update_H<T, true>(g, f, src, step_base, off, i, j, xb, threadIdx.x);
 }
 
@@ -168,7 +170,7 @@ __global__ void __launch_bounds__(32, sizeof(T) == 8 ? 18 : 32)
 k_update_E_rim(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
                SplitBox b) {
     int i, j, xb;
-    rim_task(b, blockIdx.x, i, j, xb);
+    rim_task(b, (int)blockIdx.x, i, j, xb);
     vec_update_E<T, true>(g, f, src, step_base, off, i, j, xb, threadIdx.x);
 }
 
