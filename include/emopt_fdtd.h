@@ -121,12 +121,14 @@ int FDTD_set_zchunk(FDTDHandle *h, int planes);
  * steady-state fit, probes and outputs stay float64).  Returns a status. */
 int FDTD_set_precision(FDTDHandle *h, int bits);
 
-/* Time-stepping kernel of FDTD_solve_cw: 0 = automatic (default: 5), 1 = H
- * and E kernels with one cell per thread, 3 = one fused H+E kernel per time
- * step whose warps march up z chunks (reads one field/CPML set, writes the
- * other), 5 = H and E kernels with one 2-element vector of x cells per
- * thread.  Other values fail with FDTD_ERR_ARG.  Periodic boundaries always
- * use 1. */
+/* Time-stepping kernel of FDTD_solve_cw: 0 = automatic (default: 6 in
+ * float32 when at least 60% of the 64-cell warp tasks lie in no CPML slab,
+ * else 5), 1 = H and E kernels with one cell per thread, 3 = one fused H+E
+ * kernel per time step whose warps march up z chunks (reads one field/CPML
+ * set, writes the other), 5 = H and E kernels with one 2-element vector of x
+ * cells per thread, 6 = the kernels of 5 split per half step into an
+ * interior launch (tasks in no CPML slab) and a rim launch.  Other values
+ * fail with FDTD_ERR_ARG.  Periodic boundaries always use 1. */
 int FDTD_set_kernel(FDTDHandle *h, int which);
 
 /* Page-locks (cudaHostRegister, portable) / releases host memory that is
