@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(IS_E || sizeof(T) == 8 ? 32 : 256, sizeof(T) =
 k_serve_half(GridView<T> g, Fields<T> f, SourceList<T> src, const __grid_constant__ ServeGate<T> sg,
              const long long* step_ctr) {
     const int i = (int)blockIdx.z, j = (int)blockIdx.y, xb = (int)blockIdx.x;
-    if (sizeof(T) == 4 && vecb::plain_warp<T, 1>(g, src, IS_E ? 0 : 3, i, j, xb)) {
+    if (sizeof(T) == 4 && vecb::plain_warp<T>(g, src, IS_E ? 0 : 3, i, j, xb)) {
         if (IS_E) vec_update_E<T, false, true>(g, f, src, step_ctr, 0, i, j, xb, threadIdx.x, &sg);
         else vec_update_H<T, false, true>(g, f, src, step_ctr, 0, i, j, xb, threadIdx.x, &sg);
     } else {

@@ -98,20 +98,18 @@ __device__ __forceinline__ bool sources_touch(const SourceList<T>& src, int comp
     return hit;
 }
 
-// Does the warp that updates rows j0 .. j0+NR-1 of plane i, vectors 32 xb ..
-// 32 xb + 31, touch no CPML slab and no source box of the half step
-// (comp_base 3: H sources, 0: E sources)?  Then the body built without CPML
-// and source code (GEN = false) computes the same values in the same order.
-template <typename T, int NR>
+// Does the warp that updates row j of plane i, vectors 32 xb .. 32 xb + 31,
+// touch no CPML slab and no source box of the half step (comp_base 3: H
+// sources, 0: E sources)?  Then the body built without CPML and source code
+// (GEN = false) computes the same values in the same order.
+template <typename T>
 __device__ __forceinline__ bool plain_warp(const GridView<T>& g, const SourceList<T>& src,
-                                           int comp_base, int i, int j0, int xb) {
+                                           int comp_base, int i, int j, int xb) {
     constexpr int V = V16<T>::N;
     if (slab_local(g.pml[2], i + g.pml[2].off, true) >= 0) return false;
-#pragma unroll
-    for (int r = 0; r < NR; r++)
-        if (j0 + r < g.Ny && slab_local(g.pml[1], j0 + r, false) >= 0) return false;
+    if (j < g.Ny && slab_local(g.pml[1], j, false) >= 0) return false;
     if (xb * 32 * V < g.pml[0].w0 || (xb + 1) * 32 * V - 1 >= g.pml[0].edge_max) return false;
-    return !(src.n && sources_touch<T>(src, comp_base, i, j0, j0 + NR, xb * 32 * V, (xb + 1) * 32 * V));
+    return !(src.n && sources_touch<T>(src, comp_base, i, j, j + 1, xb * 32 * V, (xb + 1) * 32 * V));
 }
 
 #ifdef FDTD_BOUNDS_CHECK

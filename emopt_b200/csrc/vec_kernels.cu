@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 32 : 256, VEC_MINB(T))
 k_update_H_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
                int i0) {
     const int i = i0 + (int)blockIdx.z, j = (int)blockIdx.y;
-    if (sizeof(T) == 4 && vecb::plain_warp<T, 1>(g, src, 3, i, j, blockIdx.x))
+    if (sizeof(T) == 4 && vecb::plain_warp<T>(g, src, 3, i, j, blockIdx.x))
         vec_update_H<T, false>(g, f, src, step_base, off, i, j, blockIdx.x, threadIdx.x);
     else
         vec_update_H<T, true>(g, f, src, step_base, off, i, j, blockIdx.x, threadIdx.x);
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(32, VEC_MINB(T))
 k_update_E_vec(GridView<T> g, Fields<T> f, SourceList<T> src, const long long* step_base, int off,
                int i0) {
     const int i = i0 + (int)blockIdx.z, j = (int)blockIdx.y;
-    if (sizeof(T) == 4 && vecb::plain_warp<T, 1>(g, src, 0, i, j, blockIdx.x))
+    if (sizeof(T) == 4 && vecb::plain_warp<T>(g, src, 0, i, j, blockIdx.x))
         vec_update_E<T, false>(g, f, src, step_base, off, i, j, blockIdx.x, threadIdx.x);
     else
         vec_update_E<T, true>(g, f, src, step_base, off, i, j, blockIdx.x, threadIdx.x);
