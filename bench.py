@@ -287,7 +287,11 @@ def run_ours(args):
     value = cell_updates_all / dev_s_max / 1e9
     fields32 = np.stack([sim._raw(c, False).copy() for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")])
 
-    # ---- e2e: public API with host buffers (materials re-uploaded each call)
+    # ---- e2e: public API with host buffers (materials re-uploaded each call);
+    # one untimed call first pays the path's one-time costs (module imports,
+    # first launches of the source-power kernel)
+    sim._materials_dirty = True
+    sim.solve_forward()
     barrier(world)
     wall = []
     for _ in range(args.steps):

@@ -960,10 +960,6 @@ fdtdb::GridView<T> make_view(FDTDHandle* h, Resident<T>& r, int set = 0) {
     g.zlo = g.zhi = 0;
     for (int c = 0; c < 4; c++) g.zhalo[c] = nullptr;
     g.chk = nullptr;
-    // prefetch two planes ahead when four planes of the nine streamed arrays
-    // (the two being updated and the two prefetched) take at most half of L2
-    const double plane_bytes = (double)h->Ny * r.px * sizeof(T);
-    g.pf = 4.0 * 9.0 * plane_bytes <= 63e6 ? 2 : 0;
 #ifdef FDTD_BOUNDS_CHECK
     g.chk = dptr<int>(r.err) + 1;
 #endif

@@ -77,7 +77,6 @@ struct GridView {
     // the neighbouring slab's boundary planes when it lives on this device
     const T* zhalo[4];
     int* chk;                      // builds with FDTD_BOUNDS_CHECK: first failed index check (else unused)
-    int pf;                        // L2 prefetch distance in planes of the vector bodies (0: none)
     PmlAxis<T> pml[3];
     const double4* step_tab;       // per step: (S_H, C_H, S_E, C_E)
 };

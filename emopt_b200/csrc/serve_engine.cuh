@@ -256,7 +256,6 @@ extern "C" int FDTD_serve_admit(FDTDServe* s, FDTDHandle* h, const FDTDSolveOpti
     fdtdb::ServeView<float>& v = s->views[slot];
     std::memset(&v, 0, sizeof(v));
     v.g = make_view<float>(h, r);
-    v.g.pf = 0;   // a request's rows are walked by many CTAs at once: no plane-ahead prefetch
     for (int c = 0; c < 6; c++) {
         v.f.c[c] = dptr<float>(r.F[0][c]);
         v.snap[0][c] = dptr<float>(r.snap[0][c]);

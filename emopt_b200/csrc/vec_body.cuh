@@ -64,21 +64,6 @@ __device__ __forceinline__ void vstore(T* p, const T (&d)[V16<T>::N]) {
     *reinterpret_cast<typename V16<T>::type*>(p) = v;
 }
 
-// L2 prefetch (GridView::pf planes ahead, 0: none).  The warp that updates
-// row j of plane i asks L2 for the same 64-cell segment of plane i + pf of
-// the arrays it streams, so that the warp which later updates that plane
-// finds them in L2 (fp32 MMI block: 119.4 instead of 121.0 us per step at
-// distance 2, fp64 199 instead of 205; distance 4 and 8 and one bulk request
-// per array gained less).  The host enables it only when the prefetched
-// planes fit in L2 beside the planes being updated (make_view).
-
-// p: first cell of the warp's segment; `room` cells of the row's pitch remain
-// from there, so no request leaves the row.
-template <typename T>
-__device__ __forceinline__ void l2_prefetch(const T* p, int lane, int room) {
-    if (2 * lane < room) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p + 2 * lane));
-}
-
 // Does a source box with a non-zero component among comp_base..comp_base+2
 // touch rows [j0, j1), columns [k0, k1) of plane i?
 template <typename T>
@@ -206,12 +191,6 @@ __device__ __forceinline__ void h_load(const GridView<T>& g, const Fields<T>& f,
 #endif
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = GEN && (xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max);
-
-    if (g.pf > 0 && i + g.pf < Nz && xb * 32 * V < g.Nx && j < Ny) {
-        const long long q = (long long)(i + g.pf) * g.plane + (long long)j * px + xb * 32 * V;
-#pragma unroll
-        for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
-    }
 
     // a served request's state and capture flag, read with the fields
     t.sstate = SERVE_RUN;
@@ -411,14 +390,6 @@ __device__ __forceinline__ void e_load(const GridView<T>& g, const Fields<T>& f,
     // does any lane of the warp touch an x slab?  (the same for all lanes)
     const bool xw = GEN && (xb * 32 * V < PX.w0 || (xb + 1) * 32 * V - 1 >= PX.edge_max);
     const bool lossy = g.aE[0] != nullptr;
-
-    if (g.pf > 0 && i + g.pf < g.Nz && xb * 32 * V < g.Nx && j < Ny) {
-        const long long q = (long long)(i + g.pf) * g.plane + (long long)j * px + xb * 32 * V;
-#pragma unroll
-        for (int c = 0; c < 6; c++) vecb::l2_prefetch<T>(f.c[c] + q, lane, px - xb * 32 * V);
-#pragma unroll
-        for (int c = 0; c < 3; c++) vecb::l2_prefetch<T>(g.bE[c] + q, lane, px - xb * 32 * V);
-    }
 
     t.sstate = SERVE_RUN;
     if (SERVE) t.sstate = __ldg(sg->state);

@@ -591,8 +591,34 @@ class FDTD(MaxwellSolver):
               self._Hx_fwd_t1, self._Hy_fwd_t1, self._Hz_fwd_t1]
         self._solve(t0, t1, self._sources)
         self.update_saved_fields()
-        self._source_power = self.get_source_power()
+        self._source_power = self._forward_source_power()
         self.forward_count += 1
+
+    def _forward_source_power(self):
+        """The source power of the forward fields for ``source_power``: the
+        Poynting sums of ``get_source_power`` (the same planes, components
+        and interpolation) on the GPU (fieldops.source_power, fixed-order fp64
+        sums) from the six grown plane blocks of the phasors, which agrees
+        with the host form to ~1e-13 relative and takes a few ms instead of
+        tens; the host form when a plane holds no cells."""
+        from . import adjoint as A
+        from . import fieldops as FO
+        import torch
+        planes = A.source_power_planes(self)
+        shape = (self._Nz, self._Ny, self._Nx)
+        d = (self._dx, self._dy, self._dz)
+        grown = [FO.grow_domain(dom, shape, d) for dom, _, _ in planes]
+        if any(g.i2 <= g.i1 or g.j2 <= g.j1 or g.k2 <= g.k1 for g in grown) or \
+                any(dom.i2 <= dom.i1 or dom.j2 <= dom.j1 or dom.k2 <= dom.k1 for dom, _, _ in planes):
+            return self.get_source_power()
+        dev = self._torch_device()
+        raws = []
+        for g in grown:
+            blk = np.stack([self._raw(c, False)[g.i1:g.i2, g.j1:g.j2, g.k1:g.k2]
+                            for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")])
+            raws.append(torch.as_tensor(blk).to(dev))
+        with torch.no_grad():
+            return float(FO.source_power(raws, planes, grown, self))
 
     def solve_adjoint(self):
         """Adjoint CW solve with the adjoint sources (``emopt/fdtd.py:1252-1300``)."""

@@ -167,3 +167,15 @@ def test_source_power_gradient_matches_autograd(bc):
     for a, b in zip(g1, g2):
         scale = float(torch.abs(b).max())
         assert float(torch.abs(a - b).max()) <= 1e-12 * max(scale, 1.0)
+
+
+@pytest.mark.parametrize("bc", ["000", "HE0"])
+def test_solve_forward_source_power_matches_host_form(bc):
+    """FDTD.solve_forward fills source_power from the phasors' plane blocks on
+    the GPU; it equals FDTD.get_source_power (host numpy) to 1e-12."""
+    p = P.random_box(5, shape=POWER_SHAPE, w_pml=POWER_PML, bc=bc, fixed_steps=200, n_sources=2)
+    sim = P.make_solver(p, precision="fp64")
+    sim.solve_forward()
+    ref = sim.get_source_power()
+    assert ref != 0.0
+    assert sim.source_power == pytest.approx(ref, rel=1e-12, abs=1e-14 * abs(ref))
