@@ -8,13 +8,15 @@ figure of merit on an output plane normalised by the source power
 (fomutils.ModeMatch, power_norm_dFdx_3D), and the reference's gradient
 protocol: the adjoint gradient from FDTD.calc_ydAx on the updated boxes
 against one-sided finite differences of the figure of merit, total relative
-error below the reference's 1% warning threshold.  Fixed step counts make
-the figure of merit a smooth function of the parameters."""
+error below the reference's 1% warning threshold.  The multi-objective
+driver (emopt/adjoint_method.py:723-929) combines two such objectives at two
+wavelengths, each on its own GPU solver.  Fixed step counts make the
+figures of merit smooth functions of the parameters."""
 import numpy as np
 import pytest
 
 from emopt_b200 import grid as G
-from emopt_b200.adjoint_method import AdjointMethodPNF3D
+from emopt_b200.adjoint_method import AdjointMethodMO, AdjointMethodPNF3D
 from emopt_b200.fdtd import FDTD
 from emopt_b200.fomutils import ModeMatch
 from emopt_b200.misc import DomainCoordinates
@@ -60,8 +62,8 @@ class TwoBlocks(AdjointMethodPNF3D):
         return np.zeros(len(params))
 
 
-def _setup():
-    sim = FDTD(X, Y, Z, D, D, D, 1.55, rtol=1e-6, precision="fp64")
+def _setup(wavelength=1.55):
+    sim = FDTD(X, Y, Z, D, D, D, wavelength, rtol=1e-6, precision="fp64")
     sim.set_pml_cells([8, 8, 8, 8, 8, 8])
     sim.fixed_steps = 2500
     eps = G.StructuredMaterial3D(sim.X, sim.Y, sim.Z, D, D, D)
@@ -103,6 +105,32 @@ def test_check_gradient_of_a_power_normalised_mode_match():
     am = TwoBlocks(sim, rects, plane, mode)
     params = np.array([3.2, 2.6])
     err, g_fd, g_am = am.check_gradient(params, plot=False, verbose=False, return_gradients=True,
+                                        fd_step=1e-4)
+    print("finite differences", g_fd, "adjoint", g_am, "total relative error %.3e" % err)
+    assert np.all(np.abs(g_fd) > 0)
+    assert err < 1e-2
+
+
+class Broadband(AdjointMethodMO):
+    """The mean of the objectives at several wavelengths."""
+
+    def calc_total_fom(self, foms):
+        return float(np.mean(foms))
+
+    def calc_total_gradient(self, foms, grads):
+        return np.mean(np.array(grads), axis=0)
+
+
+def test_check_gradient_of_a_two_wavelength_objective():
+    ams = []
+    for wl in (1.50, 1.60):
+        sim, rects, plane, mode = _setup(wl)
+        ams.append(TwoBlocks(sim, rects, plane, mode))
+    mo = Broadband(ams)
+    params = np.array([3.2, 2.6])
+    f = mo.fom(params.copy())
+    assert f == pytest.approx(np.mean([am.calc_fom(am.sim, params) for am in ams]), rel=1e-12)
+    err, g_fd, g_am = mo.check_gradient(params, plot=False, verbose=False, return_gradients=True,
                                         fd_step=1e-4)
     print("finite differences", g_fd, "adjoint", g_am, "total relative error %.3e" % err)
     assert np.all(np.abs(g_fd) > 0)
