@@ -103,6 +103,12 @@ def test_argument_errors_are_reported():
     assert ct.libFDTD.FDTD_set_precision(h, 16) == ct.FDTD_ERR_ARG
     assert "precision" in ct.last_error(h)[1]
     assert ct.libFDTD.FDTD_set_kernel(h, 8) == ct.FDTD_ERR_ARG
+    # the kernel ids the library keeps: auto, scalar, fused, vector, split
+    for k in (0, 1, 3, 5, 6):
+        assert ct.libFDTD.FDTD_set_kernel(h, k) == ct.FDTD_OK, k
+    for k in (2, 4, 7, -1):
+        assert ct.libFDTD.FDTD_set_kernel(h, k) == ct.FDTD_ERR_ARG, k
+    assert "kernel must be" in ct.last_error(h)[1]
     ct.libFDTD.FDTD_delete(h)
 
 
