@@ -7,11 +7,12 @@
 //
 // A request is a configured handle plus its solve options.  Admission checks
 // the engine's device-memory budget and a free slot, allocates and prepares
-// the request's resident state, and enters it into the slot tables; from the
-// next graph replay on (FDTD_serve_advance) the request advances with all
-// other active requests: the graph holds one branch per admitted request
-// (L time steps of its own launches, serve_kernels.cu) and is captured again
-// at the first replay after the set of requests changed.  A request
+// the request's resident state, enters it into the slot tables and captures
+// its L time steps of launches (serve_kernels.cu) as a CUDA graph of its own;
+// from the next replay on (FDTD_serve_advance) the request advances with all
+// other active requests: every replay launches the active requests' graphs
+// on their own streams, forked from the engine stream and joined back, so
+// nothing is captured again when other requests come or go.  A request
 // whose loop ended (converged, step budget or fixed length) stops stepping on
 // its own; FDTD_serve_collect extracts its complex fields into the handle's t0
 // arrays, fills its result and frees its memory.  Admission and collection
@@ -28,12 +29,10 @@ struct FDTDServe {
     std::vector<FDTDHandle*> slot_h;
     std::vector<double> slot_bytes;
     std::vector<long long> admitted_step;      // replay count at admission
-    cudaGraphExec_t exec = nullptr;
-    cudaGraph_t graph = nullptr;
-    bool dirty = true;                         // the graph does not hold the current requests
-    std::vector<cudaStream_t> aux;             // capture streams of the branches
-    std::vector<cudaEvent_t> join;
-    cudaEvent_t fork = nullptr;
+    std::vector<cudaGraphExec_t> slot_exec;    // per admitted request: its L steps as one graph
+    std::vector<cudaStream_t> aux;             // per slot: the stream its graph runs on
+    std::vector<cudaEvent_t> join;             // per slot: end of its part of a replay
+    cudaEvent_t fork = nullptr;                // start of a replay on the engine stream
     long long replays = 0;
     int status = FDTD_OK;
     std::string message;
@@ -88,50 +87,27 @@ double resident_bytes(const Resident<T>& r) {
     return b;
 }
 
-// One branch per admitted request, forked from the engine stream and joined
-// back: L time steps of the request's own launches.
-int serve_capture_graph(FDTDServe* s) {
-    if (s->exec) { cudaGraphExecDestroy(s->exec); s->exec = nullptr; }
-    if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
-    std::vector<int> act;
-    for (int q = 0; q < s->cap; q++)
-        if (s->slot_h[q]) act.push_back(q);
-    s->dirty = false;
-    if (act.empty()) return FDTD_OK;
-    while (s->aux.size() < act.size()) {
-        cudaStream_t b = nullptr;
-        cudaEvent_t ev = nullptr;
-        SCK(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
-        s->aux.push_back(b);
-        SCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        s->join.push_back(ev);
+// Slot q's L time steps of launches, captured once on the slot's stream.
+int serve_capture_request(FDTDServe* s, int q) {
+    if (!s->aux[q]) {
+        SCK(cudaStreamCreateWithFlags(&s->aux[q], cudaStreamNonBlocking));
+        SCK(cudaEventCreateWithFlags(&s->join[q], cudaEventDisableTiming));
     }
-    SCK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaEventRecord(s->fork, s->stream);
-    for (size_t k = 0; k < act.size() && e == cudaSuccess; k++) {
-        cudaStream_t b = s->aux[k];
-        e = cudaStreamWaitEvent(b, s->fork, 0);
-        for (int q = 0; q < s->L && e == cudaSuccess; q++)
-            e = fdtdb::launch_serve_request_step<float>(s->views[act[k]], s->d_ctl + act[k], b);
-        if (e == cudaSuccess) e = cudaEventRecord(s->join[k], b);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s->stream, s->join[k], 0);
-    }
+    SCK(cudaStreamBeginCapture(s->aux[q], cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int n = 0; n < s->L && e == cudaSuccess; n++)
+        e = fdtdb::launch_serve_request_step<float>(s->views[q], s->d_ctl + q, s->aux[q]);
     cudaGraph_t g = nullptr;
-    cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
+    cudaError_t e2 = cudaStreamEndCapture(s->aux[q], &g);
     if (e != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
-        s->dirty = true;
         return s->cuda_fail(e, "serve step capture");
     }
-    if (e2 != cudaSuccess) {
-        s->dirty = true;
-        return s->cuda_fail(e2, "cudaStreamEndCapture");
-    }
-    s->graph = g;
-    e = cudaGraphInstantiate(&s->exec, g, 0);
+    if (e2 != cudaSuccess) return s->cuda_fail(e2, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&s->slot_exec[q], g, 0);
+    cudaGraphDestroy(g);   // the executable graph holds what it needs
     if (e != cudaSuccess) {
-        s->exec = nullptr;
-        s->dirty = true;
+        s->slot_exec[q] = nullptr;
         return s->cuda_fail(e, "cudaGraphInstantiate");
     }
     return FDTD_OK;
@@ -167,6 +143,9 @@ extern "C" FDTDServe* FDTD_serve_new(int device, double budget_bytes, int max_re
     }
     s->views.assign(s->cap, fdtdb::ServeView<float>());
     s->slot_h.assign(s->cap, nullptr);
+    s->slot_exec.assign(s->cap, nullptr);
+    s->aux.assign(s->cap, nullptr);
+    s->join.assign(s->cap, nullptr);
     s->slot_bytes.assign(s->cap, 0);
     s->admitted_step.assign(s->cap, 0);
     std::memset(s->h_ctl, 0, sizeof(fdtdb::ServeCtl) * s->cap);
@@ -283,11 +262,14 @@ extern "C" int FDTD_serve_admit(FDTDServe* s, FDTDHandle* h, const FDTDSolveOpti
     c.state = (Tn - 1 > last) ? fdtdb::SERVE_TAIL : fdtdb::SERVE_RUN;
     SCK(cudaMemcpyAsync(s->d_ctl + slot, &c, sizeof(c), cudaMemcpyDefault, s->stream));
     SCK(cudaStreamSynchronize(s->stream));
+    if (serve_capture_request(s, slot) != FDTD_OK) {
+        r.release_all();
+        return -s->status;
+    }
     s->slot_h[slot] = h;
     s->slot_bytes[slot] = resident_bytes(r);
     s->used += s->slot_bytes[slot];
     s->admitted_step[slot] = s->replays;
-    s->dirty = true;
     s->status = FDTD_OK;
     s->message.clear();
     return slot;
@@ -301,8 +283,14 @@ extern "C" int FDTD_serve_advance(FDTDServe* s) {
     NvtxRange range("FDTD_serve_advance");
     if (!s->d_ctl) return -s->fail(FDTD_ERR_CUDA, "engine not initialised");
     SCK(cudaSetDevice(s->device));
-    if (s->dirty && serve_capture_graph(s) != FDTD_OK) return -s->status;
-    if (s->exec) SCK(cudaGraphLaunch(s->exec, s->stream));
+    SCK(cudaEventRecord(s->fork, s->stream));
+    for (int q = 0; q < s->cap; q++) {
+        if (!s->slot_h[q] || !s->slot_exec[q]) continue;
+        SCK(cudaStreamWaitEvent(s->aux[q], s->fork, 0));
+        SCK(cudaGraphLaunch(s->slot_exec[q], s->aux[q]));
+        SCK(cudaEventRecord(s->join[q], s->aux[q]));
+        SCK(cudaStreamWaitEvent(s->stream, s->join[q], 0));
+    }
     SCK(cudaMemcpyAsync(s->h_ctl, s->d_ctl, sizeof(fdtdb::ServeCtl) * s->cap, cudaMemcpyDefault, s->stream));
     SCK(cudaStreamSynchronize(s->stream));
     s->replays++;
@@ -328,7 +316,6 @@ extern "C" int FDTD_serve_collect(FDTDServe* s, FDTDHandle** done, FDTDSolveResu
     if (!s) return -FDTD_ERR_ARG;
     SCK(cudaSetDevice(s->device));
     int k = 0;
-    bool changed = false;
     for (int q = 0; q < s->cap && k < max; q++) {
         FDTDHandle* h = s->slot_h[q];
         if (!h || s->h_ctl[q].state != fdtdb::SERVE_DONE) continue;
@@ -378,13 +365,15 @@ extern "C" int FDTD_serve_collect(FDTDServe* s, FDTDHandle** done, FDTDSolveResu
         s->h_ctl[q].capture = 0;
         SCK(cudaMemcpyAsync(s->d_ctl + q, &s->h_ctl[q], sizeof(fdtdb::ServeCtl), cudaMemcpyDefault, s->stream));
         SCK(cudaStreamSynchronize(s->stream));
+        if (s->slot_exec[q]) {
+            cudaGraphExecDestroy(s->slot_exec[q]);
+            s->slot_exec[q] = nullptr;
+        }
         r.release_all();
         s->used -= s->slot_bytes[q];
         s->slot_bytes[q] = 0;
         s->slot_h[q] = nullptr;
-        changed = true;
     }
-    if (changed) s->dirty = true;
     return k;
 }
 
@@ -403,10 +392,9 @@ extern "C" void FDTD_serve_delete(FDTDServe* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (int q = 0; q < s->cap; q++)
         if (s->slot_h[q]) s->slot_h[q]->r32.release_all();
-    if (s->exec) cudaGraphExecDestroy(s->exec);
-    if (s->graph) cudaGraphDestroy(s->graph);
-    for (auto b : s->aux) cudaStreamDestroy(b);
-    for (auto ev : s->join) cudaEventDestroy(ev);
+    for (auto x : s->slot_exec) if (x) cudaGraphExecDestroy(x);
+    for (auto b : s->aux) if (b) cudaStreamDestroy(b);
+    for (auto ev : s->join) if (ev) cudaEventDestroy(ev);
     if (s->fork) cudaEventDestroy(s->fork);
     if (s->d_ctl) cudaFree(s->d_ctl);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);

@@ -5,11 +5,10 @@
 // steps and its events kernel.  The half steps are the single-solve vector
 // kernels' (vec_body.cuh, one single-warp CTA per 32-vector row segment, in
 // plane order), with the request's grid view, fields and sources in the
-// kernel parameters; the engine captures the chains of all admitted requests
-// as parallel branches of one CUDA graph of L steps, so the requests run side
-// by side and each walks its own grid in order (the L2 reuse of the
-// single-solve kernels).  The graph is captured again whenever a request is
-// admitted or retired.
+// kernel parameters; the engine captures each admitted request's chain of L
+// steps as a CUDA graph of its own and replays the active requests' graphs
+// on their own streams, so the requests run side by side and each walks its
+// own grid in order (the L2 reuse of the single-solve kernels).
 //   k_serve_half (H, then E) -- the half step, gated by the request's loop
 //       state (a finished request stores nothing until it is collected); in
 //       a step that follows a capture event the H half step also writes the
